@@ -1,0 +1,30 @@
+"""Loading of the golden fixtures produced by tests/golden/make_golden.py."""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+STEP_CASES = ("perturbed_1inst", "walls_2inst", "tall_1inst")
+
+
+def load(case):
+    return dict(np.load(os.path.join(GOLDEN, f"{case}.npz")))
+
+
+def n_instances(d):
+    return len(d["param_actuation"])
+
+
+def instance_params(d, m):
+    return dict(actuation=float(d["param_actuation"][m]), contraction=float(d["param_contraction"][m]),
+                freq=float(d["param_freq"][m]), payload_density=float(d["param_payload_density"][m]))
+
+
+def dense_grid(d, cp, m):
+    nx, ny = int(d["n_grid"]), int(d["n_grid_y"])
+    gm = np.zeros(nx * ny, np.float32)
+    gv = np.zeros((nx * ny, 2), np.float32)
+    idx = d[f"s{cp}_{m}_grid_idx"]
+    gm[idx] = d[f"s{cp}_{m}_grid_m"]
+    gv[idx] = d[f"s{cp}_{m}_grid_v"]
+    return gv.reshape(nx, ny, 2), gm.reshape(nx, ny)

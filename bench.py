@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the batched MLS-MPM substep (particle-steps/s).
+
+Workload (one bench step): 32 jellyfish instances per GPU, 80,000 particle
+slots each (about 62K live: water lattice + robot from a seeded genome), 128^2
+grid, FP32, advanced by ``--substeps`` (default 1,000) substeps through the
+batched path.  Genomes are drawn from an isotropic Gaussian (sigma = 0.3 of
+each gene's range) around the bound midpoint and clipped, per rank seed.
+Inputs are synthetic (no reference datasets exist for this path).
+
+``value`` is live particles x substeps / device time of the timed steps
+(CUDA events on the engine's stream, max over ranks), inputs resident in HBM.
+``e2e`` repeats the workload through the public API with host buffers: every
+step loads each instance from pinned host memory, runs the episode with
+``run_headless`` and reads the (M, 5) result back.  ``roofline`` rates the
+dominant kernel (the batched chunk kernel) at 100 algorithmic bytes per live
+particle-substep (x, v, C, F read and written, material read) against the
+measured HBM copy bandwidth.  ``cpu_baseline`` times the CPU oracle (a
+restatement of the reference's substep) on the host cores.  ``plain`` times
+the plain per-instance launch path on the same inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+ALGO_BYTES = 100  # bytes per live particle-substep: (x,v,C,F) 48 read + 48 write, material 4
+METRIC = "particle-steps/s @32x80K, 128^2 (batched)"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--substeps", type=int, default=1000, help="substeps per bench step")
+    ap.add_argument("--instances", type=int, default=32, help="instances per GPU")
+    ap.add_argument("--slots", type=int, default=80000)
+    ap.add_argument("--resort", type=int, default=16)
+    ap.add_argument("--block", type=int, default=512)
+    ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
+    return ap.parse_args()
+
+
+def make_inputs(M, slots, seed):
+    from jellyfih_b200 import tank
+    genomes = tank.gaussian_genomes(M, seed)
+    out = []
+    for g in genomes:
+        pos, mat, fib, st = tank.fill_tank(g, slots)
+        c, f = tank.timing_params(g)
+        out.append((pos, mat, fib, c, f, st))
+    return out
+
+
+def load_all(engine, inputs):
+    for m, (pos, mat, fib, c, f, st) in enumerate(inputs):
+        engine.load(m, pos, mat, fib)
+    engine.set_params(contraction=[i[3] for i in inputs], freq=[i[4] for i in inputs])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for name, val in zip(self.NAMES, f[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_particle_step():
+    p = os.path.join(HERE, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("chunk_kernel_dram_bytes_per_live_particle_substep")
+    return None
+
+
+def cpu_baseline(inputs, target_s=12.0):
+    """The CPU oracle on all host cores (OpenMP over instances), a bounded sample."""
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import oracle as O
+    insts, states = [], []
+    for pos, mat, fib, c, f, st in inputs:
+        insts.append(O.Instance(contraction=c, freq=f))
+        states.append(O.new_state(pos, mat, fib))
+    live = sum(int((i[1] >= 0).sum()) for i in inputs)
+    t0 = time.perf_counter()
+    t = O.run_batch(insts, states, np.float32(0), 2)
+    probe = time.perf_counter() - t0
+    n = int(max(2, min(2000, target_s / max(probe / 2, 1e-6))))
+    t0 = time.perf_counter()
+    O.run_batch(insts, states, t, n)
+    el = time.perf_counter() - t0
+    return {"value": live * n / el, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "kind": "port",
+            "sample": f"{len(inputs)} instances x {n} substeps of the same workload on the CPU oracle "
+                      f"({el:.1f} s)"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU oracle (the reference's substep restated; Taichi
+    is not installed) on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import oracle as O
+    inputs = make_inputs(args.instances, args.slots, 1000)
+    insts = [O.Instance(contraction=i[3], freq=i[4]) for i in inputs]
+    states = [O.new_state(i[0], i[1], i[2]) for i in inputs]
+    live = sum(int((i[1] >= 0).sum()) for i in inputs)
+    t = np.float32(0)
+    t0 = time.perf_counter()
+    t = O.run_batch(insts, states, t, 1)
+    probe = time.perf_counter() - t0
+    budget = 120.0  # seconds for warmup + timed steps
+    per_step = max(1, int(budget / max(args.steps + args.warmup, 1) / max(probe, 1e-6)))
+    per_step = min(per_step, args.substeps)
+    for _ in range(args.warmup):
+        t = O.run_batch(insts, states, t, per_step)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t = O.run_batch(insts, states, t, per_step)
+    el = time.perf_counter() - t0
+    value = live * per_step * args.steps / el
+    sample = (f"{args.instances} instances x {per_step} substeps per step (bounded sample of the "
+              f"{args.substeps}-substep step)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"{args.instances} instances x {args.slots} slots, 128^2 grid, "
+                                   "CPU oracle of the reference substep", "instances": args.instances,
+                       "slots": args.slots, "live_particles": live, "substeps_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allreduce(x, op):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    from jellyfih_b200 import Engine, InstanceSpec
+    M, S, K, W = args.instances, args.substeps, args.steps, args.warmup
+    inputs = make_inputs(M, args.slots, 1000 + rank)
+    live = sum(int((i[1] >= 0).sum()) for i in inputs)
+    spec = InstanceSpec(args.slots)
+    engine = Engine([spec] * M, path="batched", device=local, resort_interval=args.resort,
+                    block_threads=args.block)
+    stream = torch.cuda.Stream()
+    engine.set_stream(stream)
+    load_all(engine, inputs)
+    engine.time = 0.0
+
+    for _ in range(W):
+        engine.step(S)
+    engine.sync()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    engine.set_kernel_timing(True)
+    launches0 = engine.kernel_launches
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(K):
+            engine.step(S)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    kt = engine.kernel_timing()
+    engine.set_kernel_timing(False)
+    gpu_launches = engine.kernel_launches - launches0
+    flags = engine.error_flags()
+    ms_max = allreduce(ms, dist.ReduceOp.MAX if world > 1 else None)
+    live_total = allreduce(float(live), dist.ReduceOp.SUM if world > 1 else None)
+    value = live_total * S * K / (ms_max / 1e3)
+
+    # dominant kernel roofline: algorithmic bytes per chunk launch / mean launch time
+    peak, peak_kind = peaks()
+    chunk_substeps = S * K / max(kt["step_launches"], 1)
+    bytes_per_launch = live * chunk_substeps * ALGO_BYTES
+    mean_launch_s = kt["step_ms"] / max(kt["step_launches"], 1) / 1e3
+    achieved = bytes_per_launch / mean_launch_s / 1e9
+    tpps = traffic_per_particle_step()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tpps * live * chunk_substeps) if tpps else None,
+                "kernel": "chunk_kernel", "algorithmic_bytes_per_launch": bytes_per_launch,
+                "mean_launch_ms": mean_launch_s * 1e3, "launches": kt["step_launches"],
+                "step_kernel_share": kt["step_ms"] / ms if ms > 0 else None,
+                "sort_ms": kt["sort_ms"], "sort_launches": kt["sort_launches"]}
+
+    extras = {}
+    if not args.no_extras:
+        # e2e through the public API: host (pinned) inputs in, (M, 5) results out, every step
+        pinned = []
+        for pos, mat, fib, c, f, st in inputs:
+            hp = torch.from_numpy(pos).pin_memory().numpy()
+            hm = torch.from_numpy(mat).pin_memory().numpy()
+            hf = torch.from_numpy(fib).pin_memory().numpy()
+            pinned.append((hp, hm, hf, c, f))
+        h2d = sum(a.nbytes + b.nbytes + c.nbytes for a, b, c, _, _ in pinned)
+        e2e_steps = max(2, K // 4)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for m, (hp, hm, hf, c, f) in enumerate(pinned):
+                engine.load(m, hp, hm, hf)
+            engine.set_params(contraction=[p[3] for p in pinned], freq=[p[4] for p in pinned])
+            res = engine.run_headless(S)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        barrier()
+        el = allreduce(el, dist.ReduceOp.MAX if world > 1 else None)
+        extras["e2e"] = {"value": live_total * S * e2e_steps / el, "unit": UNIT,
+                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": res.nbytes + 2 * 6 * 8 * M,
+                         "steps": e2e_steps, "api": "Engine.load + Engine.run_headless (C ABI)"}
+        if world > 1:
+            allres = [torch.zeros((M, 5), dtype=torch.float64, device="cuda") for _ in range(world)]
+            dist.all_gather(allres, torch.from_numpy(res).cuda())
+            extras["e2e"]["gathered_results"] = int(sum(r.shape[0] for r in allres))
+
+        # plain per-instance launch path on the same inputs (BASELINE: batched vs plain)
+        plain = Engine([spec] * M, path="plain", device=local)
+        plain.set_stream(stream)
+        load_all(plain, inputs)
+        P = 50
+        plain.step(5)
+        plain.sync()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        plain.step(P)
+        p1.record(stream)
+        p1.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain.close()
+        plain_value = live * P / (pms / 1e3) * world
+        extras["plain"] = {"value": plain_value, "unit": UNIT, "substeps": P,
+                           "ms_per_substep": pms / P,
+                           "batched_over_plain": value / plain_value}
+
+        if rank == 0 and world == 1:
+            extras["cpu_baseline"] = cpu_baseline(inputs)
+
+    engine.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"batched {M} instances x {args.slots} slots per GPU, 128^2 grid, "
+                                       f"FP32, {S} substeps per step",
+                           "instances_per_gpu": M, "slots": args.slots, "live_particles": int(live_total),
+                           "substeps_per_step": S, "resort_interval": args.resort,
+                           "block_threads": args.block,
+                           "l2": "inputs larger than L2: particle state plus sort buffers ~260 MB per GPU",
+                           "path": "batched"},
+                "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": gpu_launches,
+                "nonfinite_instances": int(np.count_nonzero(flags)),
+                "fwd_bwd_over_fwd": None}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,148 @@
+/*
+ * jellyfih.h -- C ABI of the B200 MLS-MPM engine (libjellyfih.so).
+ *
+ * The engine replaces the Taichi-backed module mpm_sim.py of jellyfih: one
+ * handle owns every device buffer for its lifetime, as mpm_sim.py owns its
+ * global fields from import (mpm_sim.py:86-142).  Plain pointers and sizes
+ * only; host arrays use the reference's field layouts:
+ *   positions, velocities, fibres  float[n][2]      (x, v, fiber_dir)
+ *   C, F                           float[n][2][2]   row-major
+ *   material                       int32[n]         -1 = dead slot
+ *   grid_v                         float[nx][ny][2] grid_m float[nx][ny]
+ *
+ * Every call returns JF_OK (0) or an error code; jf_last_error() gives the
+ * message.  A handle is not thread-safe.  Work is queued on the engine's CUDA
+ * stream; calls that return host data synchronise that stream.
+ */
+#ifndef JELLYFIH_H
+#define JELLYFIH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JF_OK 0
+#define JF_ERR_INVALID 1      /* bad argument, shape or state */
+#define JF_ERR_CUDA 2         /* a CUDA call failed */
+#define JF_ERR_NONFINITE 3    /* a particle state became NaN/Inf */
+#define JF_ERR_UNSUPPORTED 4  /* configuration outside what the chosen path supports */
+
+#define JF_PATH_PLAIN 0       /* one instance per launch sequence (reference structure) */
+#define JF_PATH_BATCHED 1     /* all instances in one persistent cluster launch per chunk */
+
+#define JF_FLAG_GLOW 1u       /* keep the render-only visual_glow field up to date */
+
+typedef struct jf_engine jf_engine;
+
+/* One simulation instance: slot capacity and grid (mpm_sim.py:11-19). */
+typedef struct {
+  int32_t n_slots;        /* particle slots (n_particles) */
+  int32_t n_grid;         /* grid nodes along x (n_grid; dx = 1 / n_grid) */
+  int32_t n_grid_y;       /* grid nodes along y (n_grid_y) */
+  float domain_height;    /* physical height of the tank (domain_height) */
+} jf_instance_desc;
+
+typedef struct {
+  int32_t n_instances;                  /* n_instances */
+  const jf_instance_desc* instances;    /* n_instances entries */
+  double dt;                            /* substep (mpm_sim.py:19), 0 = 2e-5 */
+  int32_t path;                         /* JF_PATH_* */
+  uint32_t flags;                       /* JF_FLAG_* */
+  int32_t device;                       /* CUDA device ordinal */
+  int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 16 */
+  int32_t block_threads;                /* batched: threads per CTA, 0 = 512 */
+} jf_config;
+
+/* Engine life cycle.  Replaces the import-time allocation of mpm_sim.py:86-149;
+ * per-instance parameters start at the reference defaults (actuation 500,
+ * contraction 0.2, frequency multiplier 1.0, payload density 2.5). */
+int jf_create(const jf_config* cfg, jf_engine** out);
+int jf_destroy(jf_engine* e);
+const char* jf_last_error(const jf_engine* e);
+const char* jf_version(void);
+
+/* Stream the engine queues work on (a cudaStream_t); NULL restores the
+ * engine's own stream. */
+int jf_set_stream(jf_engine* e, void* stream);
+
+/* Reset instance `m` from host arrays of n <= n_slots particles
+ * (load_particles / _load_particles_kernel, mpm_sim.py:715-736): x, material
+ * and fibre from the arrays (fiber == NULL gives (0, 1)), v = 0, F = I, C = 0,
+ * Jp = 1; slots n..n_slots-1 become dead. */
+int jf_load_instance(jf_engine* e, int32_t m, const float* pos, const int32_t* material,
+                     const float* fiber, int32_t n);
+
+/* Per-instance parameters, host arrays of n_instances floats; NULL leaves a
+ * parameter unchanged (instance_actuation, instance_act_contraction,
+ * instance_freq, instance_payload_density; mpm_sim.py:116-149). */
+int jf_set_params(jf_engine* e, const float* actuation, const float* contraction,
+                  const float* freq, const float* payload_density);
+int jf_get_params(const jf_engine* e, float* actuation, float* contraction, float* freq,
+                  float* payload_density);
+
+/* sim_time[None] (mpm_sim.py:95), an FP32 running sum advanced by dt per substep. */
+int jf_set_time(jf_engine* e, float t);
+int jf_get_time(const jf_engine* e, float* t);
+
+/* n substeps of every instance (n calls of substep(), mpm_sim.py:153-340). */
+int jf_step(jf_engine* e, int64_t n_steps);
+int jf_sync(jf_engine* e);
+
+/* get_payload_stats (mpm_sim.py:764-777): out[n_instances][3] =
+ * [com_y, com_x, count] of the payload (material 2), zeros without payload.
+ * Sums are accumulated on the GPU in FP64. */
+int jf_payload_stats(jf_engine* e, double* out);
+
+/* _get_stats_any (mpm_sim.py:779-800): payload CoM where present, else the
+ * CoM of jelly + muscle (materials 1 and 3). */
+int jf_stats_any(jf_engine* e, double* out);
+
+/* The FP64 sums behind the CoM (clear_fitness_buffer + compute_payload_stats
+ * / compute_body_stats, mpm_sim.py:740-762): out[n_instances][6] =
+ * [payload sum_y, payload count, payload sum_x, body sum_y, body count,
+ * body sum_x], body = materials 1 and 3. */
+int jf_stats_raw(jf_engine* e, double* out);
+
+/* run_batch_headless (mpm_sim.py:802-834): time reset to 0, CoM before,
+ * `steps` substeps, CoM after; out[n_instances][5] = [init_y, init_x,
+ * final_y, final_x, valid] with valid = final_y >= 0.01. */
+int jf_run_headless(jf_engine* e, int64_t steps, double* out);
+
+/* Particle fields of instance m in slot order (field.to_numpy()); any
+ * pointer may be NULL.  x, v, fiber: [n_slots][2]; C, F: [n_slots][4]. */
+int jf_read_particles(jf_engine* e, int32_t m, float* x, float* v, float* C, float* F,
+                      int32_t* material, float* Jp, float* glow, float* fiber);
+
+/* Overwrite particle fields of instance m from slot-order host arrays
+ * (field.from_numpy()); NULL leaves a field unchanged. */
+int jf_write_particles(jf_engine* e, int32_t m, const float* x, const float* v, const float* C,
+                       const float* F, const float* Jp, const float* glow);
+
+/* grid_v / grid_m of instance m after the last substep (mpm_sim.py:92-93):
+ * grid_v[nx][ny][2], grid_m[nx][ny]; either may be NULL. */
+int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m);
+
+/* Per-instance non-finite flags raised by the G2P update since the last
+ * clear (out[n_instances]). */
+int jf_error_flags(jf_engine* e, int32_t* out);
+int jf_clear_error_flags(jf_engine* e);
+
+/* Number of kernels this engine has launched. */
+int64_t jf_kernel_launches(const jf_engine* e);
+
+/* Kernel timing with CUDA events on the engine's stream.  While enabled, every
+ * step-kernel launch is bracketed by events; jf_kernel_timing synchronises and
+ * returns the summed device time (ms) and launch counts of the step kernels
+ * (batched chunk kernel, or the plain P2G / grid / G2P kernels) and of the
+ * batched re-sort kernels, accumulated since timing was enabled. */
+int jf_set_kernel_timing(jf_engine* e, int32_t enable);
+int jf_kernel_timing(jf_engine* e, double* step_ms, int64_t* step_launches, double* sort_ms,
+                     int64_t* sort_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JELLYFIH_H */

@@ -1,0 +1,616 @@
+// C-ABI entry points of libjellyfih.so (declared in include/jellyfih.h).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "jf_engine.h"
+
+cudaError_t jf_batched_prepare(jf_engine* e);
+int jf_batched_max_active_clusters(jf_engine* e, int cluster, int* out);
+
+namespace {
+
+std::string g_create_err;  // message of the last failed jf_create
+
+constexpr int kHaloRows = 4;  // batched window rows beyond the band (1 below, 3 above)
+constexpr size_t kMaxSmem = 227 * 1024;
+
+int fail(jf_engine* e, int code, const std::string& msg) {
+  if (e) e->err = msg;
+  return code;
+}
+
+int cuda_fail(jf_engine* e, cudaError_t err, const char* what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorName(err) + " (" + cudaGetErrorString(err) + ")";
+  return fail(e, JF_ERR_CUDA, msg);
+}
+
+#define JF_CK(call, what)                                   \
+  do {                                                      \
+    cudaError_t _err = (call);                              \
+    if (_err != cudaSuccess) return cuda_fail(e, _err, what); \
+  } while (0)
+
+template <class T>
+cudaError_t alloc(T** p, size_t n) {
+  return cudaMalloc((void**)p, sizeof(T) * (n > 0 ? n : 1));
+}
+
+cudaError_t alloc_particles(JfParticles& p, size_t n) {
+  cudaError_t err;
+  if ((err = alloc(&p.xv, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.C, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.F, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.mat, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.fiber, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.Jp, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.glow, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.slot, n)) != cudaSuccess) return err;
+  return cudaSuccess;
+}
+
+void free_particles(JfParticles& p) {
+  cudaFree(p.xv); cudaFree(p.C); cudaFree(p.F); cudaFree(p.mat);
+  cudaFree(p.fiber); cudaFree(p.Jp); cudaFree(p.glow); cudaFree(p.slot);
+  p = JfParticles();
+}
+
+int check_engine(const jf_engine* e) { return e ? JF_OK : JF_ERR_INVALID; }
+
+int set_device(jf_engine* e) {
+  JF_CK(cudaSetDevice(e->device), "cudaSetDevice");
+  return JF_OK;
+}
+
+int upload_params(jf_engine* e) {
+  if (!e->params_dirty) return JF_OK;
+  JF_CK(cudaMemcpyAsync(e->d_params, e->params.data(), sizeof(JfParams) * e->M,
+                        cudaMemcpyHostToDevice, e->stream),
+        "upload params");
+  JF_CK(cudaStreamSynchronize(e->stream), "upload params sync");
+  e->params_dirty = false;
+  return JF_OK;
+}
+
+// Instance m's particle arrays in engine order, copied to the host.
+struct HostInstance {
+  std::vector<float4> xv, C, F;
+  std::vector<int32_t> mat, slot;
+  std::vector<float2> fiber;
+  std::vector<float> Jp, glow;
+};
+
+int download_instance(jf_engine* e, int m, HostInstance& h) {
+  const JfInst& I = e->inst[m];
+  const size_t n = (size_t)I.n_slots;
+  h.xv.resize(n); h.C.resize(n); h.F.resize(n); h.mat.resize(n); h.slot.resize(n);
+  h.fiber.resize(n); h.Jp.resize(n); h.glow.resize(n);
+  if (n == 0) return JF_OK;
+  const int64_t o = I.p_off;
+  JF_CK(cudaMemcpyAsync(h.xv.data(), e->p.xv + o, n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream), "read xv");
+  JF_CK(cudaMemcpyAsync(h.C.data(), e->p.C + o, n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream), "read C");
+  JF_CK(cudaMemcpyAsync(h.F.data(), e->p.F + o, n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream), "read F");
+  JF_CK(cudaMemcpyAsync(h.mat.data(), e->p.mat + o, n * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream), "read mat");
+  JF_CK(cudaMemcpyAsync(h.slot.data(), e->p.slot + o, n * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream), "read slot");
+  JF_CK(cudaMemcpyAsync(h.fiber.data(), e->p.fiber + o, n * sizeof(float2), cudaMemcpyDeviceToHost, e->stream), "read fiber");
+  JF_CK(cudaMemcpyAsync(h.Jp.data(), e->p.Jp + o, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream), "read Jp");
+  JF_CK(cudaMemcpyAsync(h.glow.data(), e->p.glow + o, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream), "read glow");
+  JF_CK(cudaStreamSynchronize(e->stream), "read particles sync");
+  for (size_t k = 0; k < n; ++k) {
+    if (h.slot[k] < 0 || (size_t)h.slot[k] >= n) return fail(e, JF_ERR_CUDA, "corrupt slot permutation");
+  }
+  return JF_OK;
+}
+
+int upload_instance(jf_engine* e, int m, const HostInstance& h) {
+  const JfInst& I = e->inst[m];
+  const size_t n = (size_t)I.n_slots;
+  if (n == 0) return JF_OK;
+  const int64_t o = I.p_off;
+  JF_CK(cudaMemcpyAsync(e->p.xv + o, h.xv.data(), n * sizeof(float4), cudaMemcpyHostToDevice, e->stream), "write xv");
+  JF_CK(cudaMemcpyAsync(e->p.C + o, h.C.data(), n * sizeof(float4), cudaMemcpyHostToDevice, e->stream), "write C");
+  JF_CK(cudaMemcpyAsync(e->p.F + o, h.F.data(), n * sizeof(float4), cudaMemcpyHostToDevice, e->stream), "write F");
+  JF_CK(cudaMemcpyAsync(e->p.Jp + o, h.Jp.data(), n * sizeof(float), cudaMemcpyHostToDevice, e->stream), "write Jp");
+  JF_CK(cudaMemcpyAsync(e->p.glow + o, h.glow.data(), n * sizeof(float), cudaMemcpyHostToDevice, e->stream), "write glow");
+  JF_CK(cudaStreamSynchronize(e->stream), "write particles sync");
+  return JF_OK;
+}
+
+int stats_rows(jf_engine* e, double* out, bool any) {
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  std::vector<double> raw(6 * (size_t)e->M);
+  JF_CK(cudaMemcpyAsync(raw.data(), e->d_stats, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost,
+                        e->stream),
+        "read stats");
+  JF_CK(cudaStreamSynchronize(e->stream), "stats sync");
+  for (int m = 0; m < e->M; ++m) {
+    const double* r = &raw[6 * (size_t)m];
+    if (any && r[1] == 0) r = r + 3;  // body CoM fallback (mpm_sim.py:786-792)
+    double* o = out + 3 * (size_t)m;
+    if (r[1] > 0) {
+      o[0] = r[0] / r[1];
+      o[1] = r[2] / r[1];
+      o[2] = r[1];
+    } else {
+      o[0] = o[1] = o[2] = 0.0;
+    }
+  }
+  return JF_OK;
+}
+
+int step_impl(jf_engine* e, int64_t n) {
+  if (n < 0) return fail(e, JF_ERR_INVALID, "n_steps must be >= 0");
+  if (n == 0) return JF_OK;
+  int rc = set_device(e);
+  if (rc) return rc;
+  rc = upload_params(e);
+  if (rc) return rc;
+  cudaError_t err = (e->path == JF_PATH_BATCHED) ? jf_batched_step(e, n) : jf_plain_step(e, n);
+  if (err != cudaSuccess) return cuda_fail(e, err, "step");
+  return JF_OK;
+}
+
+// Folds recorded event pairs into the totals and returns the events to the pool.
+cudaError_t collect_timing(jf_engine* e) {
+  cudaError_t first = cudaSuccess;
+  for (int which = 0; which < 2; ++which) {
+    auto& list = which ? e->sort_events : e->step_events;
+    for (auto& pr : list) {
+      float ms = 0.0f;
+      cudaError_t err = cudaEventElapsedTime(&ms, pr.first, pr.second);
+      if (err != cudaSuccess && first == cudaSuccess) first = err;
+      (which ? e->sort_ms : e->step_ms) += ms;
+      (which ? e->sort_launches : e->step_launches) += 1;
+      e->event_pool.push_back(pr.first);
+      e->event_pool.push_back(pr.second);
+    }
+    list.clear();
+  }
+  return first;
+}
+
+}  // namespace
+
+static cudaEvent_t pool_event(jf_engine* e) {
+  if (!e->event_pool.empty()) {
+    cudaEvent_t ev = e->event_pool.back();
+    e->event_pool.pop_back();
+    return ev;
+  }
+  cudaEvent_t ev = nullptr;
+  cudaEventCreate(&ev);
+  return ev;
+}
+
+JfTimed::JfTimed(jf_engine* eng, bool sort) : e(eng), list(sort ? &eng->sort_events : &eng->step_events) {
+  if (!e->timing) return;
+  a = pool_event(e);
+  b = pool_event(e);
+  cudaEventRecord(a, e->stream);
+}
+
+JfTimed::~JfTimed() {
+  if (!e->timing || !a) return;
+  cudaEventRecord(b, e->stream);
+  list->push_back({a, b});
+}
+
+extern "C" {
+
+const char* jf_version(void) { return "jellyfih-b200 0.1"; }
+
+const char* jf_last_error(const jf_engine* e) { return e ? e->err.c_str() : g_create_err.c_str(); }
+
+int jf_create(const jf_config* cfg, jf_engine** out) {
+  if (!out) return JF_ERR_INVALID;
+  *out = nullptr;
+  if (!cfg || cfg->n_instances <= 0 || !cfg->instances) {
+    g_create_err = "config needs n_instances > 0 and an instance table";
+    return JF_ERR_INVALID;
+  }
+  if (cfg->path != JF_PATH_PLAIN && cfg->path != JF_PATH_BATCHED) {
+    g_create_err = "unknown path";
+    return JF_ERR_INVALID;
+  }
+  jf_engine* e = new jf_engine();
+  e->device = cfg->device;
+  e->M = cfg->n_instances;
+  e->dt = cfg->dt > 0 ? cfg->dt : 2e-5;
+  e->path = cfg->path;
+  e->flags = cfg->flags;
+  e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 16;
+  e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
+  auto bail = [&](int code, const std::string& msg) {
+    g_create_err = msg;
+    jf_destroy(e);
+    return code;
+  };
+  if (e->block_threads > 512 || e->block_threads % 32) return bail(JF_ERR_INVALID, "block_threads must be a multiple of 32, <= 512");
+
+  int ny_max = 0;
+  for (int m = 0; m < e->M; ++m) {
+    const jf_instance_desc& d = cfg->instances[m];
+    if (d.n_slots < 0 || d.n_grid < 8 || d.n_grid_y < 8 || !(d.domain_height > 0))
+      return bail(JF_ERR_INVALID, "instance " + std::to_string(m) + ": bad n_slots / n_grid / domain_height");
+    ny_max = std::max(ny_max, (int)d.n_grid_y);
+  }
+
+  int rc = set_device(e);
+  if (rc) return bail(rc, e->err);
+  int n_sm = 148;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, e->device);
+
+  // cluster size: grow while the launch still fits the SMs and bands keep >= 8 rows
+  e->cluster = 4;
+  if (e->path == JF_PATH_BATCHED) {
+    while (e->cluster < 16 && (int64_t)e->M * e->cluster * 2 <= n_sm &&
+           (ny_max + e->cluster * 2 - 1) / (e->cluster * 2) >= 8)
+      e->cluster *= 2;
+  }
+
+  int64_t p_off = 0, g_off = 0;
+  for (int m = 0; m < e->M; ++m) {
+    const jf_instance_desc& d = cfg->instances[m];
+    JfInst I;
+    const double nx = d.n_grid;
+    const double dx_d = 1.0 / nx;
+    const double p_vol = (dx_d * 0.5) * (dx_d * 0.5);
+    I.nx = d.n_grid;
+    I.ny = d.n_grid_y;
+    I.dcx = d.n_grid / 20;
+    I.dcy = d.n_grid_y / 20;
+    I.band_h = (d.n_grid_y + e->cluster - 1) / e->cluster;
+    I.n_slots = d.n_slots;
+    I.p_off = p_off;
+    I.g_off = g_off;
+    I.inv_dx = (float)nx;
+    I.dx = (float)dx_d;
+    I.dt = (float)e->dt;
+    I.p_mass = (float)(p_vol * 1);
+    I.stress_scale = (float)(-e->dt * p_vol * 4 * nx * nx);
+    I.c4 = (float)(4 * nx);
+    I.dtg = (float)(e->dt * 10.0);
+    I.y_hi = (float)((double)d.domain_height - 0.001);
+    e->inst.push_back(I);
+    JfParams P = {500.0f, 0.20f, 1.0f, 2.5f};  // mpm_sim.py:143-149
+    e->params.push_back(P);
+    p_off += d.n_slots;
+    g_off += (int64_t)d.n_grid * d.n_grid_y;
+    e->max_slots = std::max(e->max_slots, d.n_slots);
+    e->max_cells = std::max(e->max_cells, d.n_grid * d.n_grid_y);
+    e->win_nodes = std::max(e->win_nodes, (I.band_h + kHaloRows) * d.n_grid);
+  }
+  e->total_slots = p_off;
+  e->total_nodes = g_off;
+  if (p_off >= (int64_t)1 << 31) return bail(JF_ERR_UNSUPPORTED, "more than 2^31 particle slots");
+  if (e->path == JF_PATH_BATCHED && jf_batched_smem_bytes(e) > kMaxSmem)
+    return bail(JF_ERR_UNSUPPORTED, "grid band does not fit in shared memory (n_grid * rows too large)");
+
+  if (!e->stream) {
+    cudaError_t err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) return bail(JF_ERR_CUDA, "cudaStreamCreate failed");
+    e->own_stream = true;
+  }
+  cudaError_t err = cudaSuccess;
+  if ((err = alloc_particles(e->p, p_off)) != cudaSuccess ||
+      (err = alloc(&e->d_inst, e->M)) != cudaSuccess ||
+      (err = alloc(&e->d_params, e->M)) != cudaSuccess ||
+      (err = alloc(&e->d_grid, g_off)) != cudaSuccess ||
+      (err = alloc(&e->d_stats, 6 * (size_t)e->M)) != cudaSuccess ||
+      (err = alloc(&e->d_err, e->M)) != cudaSuccess ||
+      (err = alloc(&e->d_stage, 8 * (size_t)e->max_slots)) != cudaSuccess ||
+      (err = alloc(&e->d_stage_i, 2 * (size_t)e->max_slots)) != cudaSuccess)
+    return bail(JF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+  if (e->path == JF_PATH_BATCHED) {
+    if ((err = alloc_particles(e->q, p_off)) != cudaSuccess ||
+        (err = alloc(&e->d_keys, p_off)) != cudaSuccess ||
+        (err = alloc(&e->d_counts, (size_t)(e->max_cells + 2) * e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess)
+      return bail(JF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+    if ((err = jf_batched_prepare(e)) != cudaSuccess)
+      return bail(JF_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(err));
+    int active = 0;
+    jf_batched_max_active_clusters(e, e->cluster, &active);
+    if (active == 0)
+      return bail(JF_ERR_UNSUPPORTED, "clusters of " + std::to_string(e->cluster) + " CTAs cannot be scheduled");
+  }
+  if (cudaMemcpy(e->d_inst, e->inst.data(), sizeof(JfInst) * e->M, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(e->d_grid, 0, sizeof(float4) * std::max<int64_t>(g_off, 1)) != cudaSuccess ||
+      cudaMemset(e->d_err, 0, sizeof(int32_t) * e->M) != cudaSuccess ||
+      cudaMemset(e->p.glow, 0, sizeof(float) * std::max<int64_t>(p_off, 1)) != cudaSuccess)
+    return bail(JF_ERR_CUDA, "initial upload failed");
+  // every slot starts dead: position -1, material -1, F = I, Jp = 1
+  {
+    std::vector<float> zeros(5 * (size_t)std::max(e->max_slots, 1), 0.0f);
+    cudaMemcpy(e->d_stage + 4 * (size_t)e->max_slots, zeros.data(), sizeof(float) * e->max_slots,
+               cudaMemcpyHostToDevice);
+    for (int m = 0; m < e->M; ++m) {
+      if (jf_load_launch(e, m, 0) != cudaSuccess) return bail(JF_ERR_CUDA, "initial reset failed");
+    }
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess) return bail(JF_ERR_CUDA, "initial reset sync failed");
+  }
+  e->params_dirty = true;
+  *out = e;
+  return JF_OK;
+}
+
+int jf_destroy(jf_engine* e) {
+  if (!e) return JF_ERR_INVALID;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  free_particles(e->p);
+  free_particles(e->q);
+  cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
+  cudaFree(e->d_band); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
+  cudaFree(e->d_stage); cudaFree(e->d_stage_i);
+  for (auto& pr : e->step_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+  for (auto& pr : e->sort_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+  for (auto ev : e->event_pool) cudaEventDestroy(ev);
+  if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return JF_OK;
+}
+
+int jf_set_stream(jf_engine* e, void* stream) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(cudaStreamSynchronize(e->stream), "sync old stream");
+  if (stream) {
+    if (e->own_stream) cudaStreamDestroy(e->stream);
+    e->own_stream = false;
+    e->stream = (cudaStream_t)stream;
+  } else if (!e->own_stream) {
+    JF_CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    e->own_stream = true;
+  }
+  return JF_OK;
+}
+
+int jf_load_instance(jf_engine* e, int32_t m, const float* pos, const int32_t* material,
+                     const float* fiber, int32_t n) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  const JfInst& I = e->inst[m];
+  if (n < 0 || n > I.n_slots) return fail(e, JF_ERR_INVALID, "particle count exceeds the instance's slots");
+  if (n > 0 && (!pos || !material)) return fail(e, JF_ERR_INVALID, "positions and materials are required");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const size_t S = (size_t)e->max_slots;
+  // glow is not reset by a load (mpm_sim.py:715-727): keep it, in slot order
+  JF_CK(jf_glow_to_slot_order(e, m), "glow reorder");
+  std::vector<float> fib;
+  if (!fiber && n > 0) {
+    fib.assign(2 * (size_t)n, 0.0f);
+    for (int k = 0; k < n; ++k) fib[2 * k + 1] = 1.0f;
+    fiber = fib.data();
+  }
+  if (n > 0) {
+    JF_CK(cudaMemcpyAsync(e->d_stage, pos, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, e->stream), "stage pos");
+    JF_CK(cudaMemcpyAsync(e->d_stage + 2 * S, fiber, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, e->stream),
+          "stage fiber");
+    JF_CK(cudaMemcpyAsync(e->d_stage_i, material, sizeof(int32_t) * n, cudaMemcpyHostToDevice, e->stream),
+          "stage material");
+  }
+  JF_CK(jf_load_launch(e, m, n), "load kernel");
+  JF_CK(cudaStreamSynchronize(e->stream), "load sync");
+  e->sorted = false;
+  return JF_OK;
+}
+
+int jf_set_params(jf_engine* e, const float* actuation, const float* contraction, const float* freq,
+                  const float* payload_density) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  for (int m = 0; m < e->M; ++m) {
+    if (actuation) e->params[m].actuation = actuation[m];
+    if (contraction) e->params[m].contraction = contraction[m];
+    if (freq) e->params[m].freq = freq[m];
+    if (payload_density) e->params[m].payload_density = payload_density[m];
+  }
+  e->params_dirty = true;
+  return JF_OK;
+}
+
+int jf_get_params(const jf_engine* e, float* actuation, float* contraction, float* freq,
+                  float* payload_density) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  for (int m = 0; m < e->M; ++m) {
+    if (actuation) actuation[m] = e->params[m].actuation;
+    if (contraction) contraction[m] = e->params[m].contraction;
+    if (freq) freq[m] = e->params[m].freq;
+    if (payload_density) payload_density[m] = e->params[m].payload_density;
+  }
+  return JF_OK;
+}
+
+int jf_set_time(jf_engine* e, float t) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  e->t = t;
+  return JF_OK;
+}
+
+int jf_get_time(const jf_engine* e, float* t) {
+  if (check_engine(e) || !t) return JF_ERR_INVALID;
+  *t = e->t;
+  return JF_OK;
+}
+
+int jf_step(jf_engine* e, int64_t n_steps) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  return step_impl(e, n_steps);
+}
+
+int jf_sync(jf_engine* e) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(cudaStreamSynchronize(e->stream), "sync");
+  return JF_OK;
+}
+
+int jf_payload_stats(jf_engine* e, double* out) {
+  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  return stats_rows(e, out, false);
+}
+
+int jf_stats_any(jf_engine* e, double* out) {
+  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  return stats_rows(e, out, true);
+}
+
+int jf_stats_raw(jf_engine* e, double* out) {
+  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  JF_CK(cudaMemcpyAsync(out, e->d_stats, sizeof(double) * 6 * e->M, cudaMemcpyDeviceToHost, e->stream),
+        "read stats");
+  JF_CK(cudaStreamSynchronize(e->stream), "stats sync");
+  return JF_OK;
+}
+
+int jf_run_headless(jf_engine* e, int64_t steps, double* out) {
+  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  e->t = 0.0f;
+  std::vector<double> initial(3 * (size_t)e->M), final_(3 * (size_t)e->M);
+  if ((rc = stats_rows(e, initial.data(), true))) return rc;
+  if ((rc = step_impl(e, steps))) return rc;
+  if ((rc = stats_rows(e, final_.data(), true))) return rc;
+  for (int m = 0; m < e->M; ++m) {
+    const double* a = &initial[3 * (size_t)m];
+    const double* b = &final_[3 * (size_t)m];
+    double* o = out + 5 * (size_t)m;
+    o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
+    if (a[2] > 0 && b[2] > 0) {
+      o[0] = a[0]; o[1] = a[1]; o[2] = b[0]; o[3] = b[1];
+      o[4] = (b[0] < 0.01) ? 0.0 : 1.0;
+    }
+  }
+  return JF_OK;
+}
+
+int jf_read_particles(jf_engine* e, int32_t m, float* x, float* v, float* C, float* F, int32_t* material,
+                      float* Jp, float* glow, float* fiber) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  int rc = set_device(e);
+  if (rc) return rc;
+  HostInstance h;
+  if ((rc = download_instance(e, m, h))) return rc;
+  const size_t n = h.slot.size();
+  for (size_t k = 0; k < n; ++k) {
+    const size_t s = (size_t)h.slot[k];
+    if (x) { x[2 * s] = h.xv[k].x; x[2 * s + 1] = h.xv[k].y; }
+    if (v) { v[2 * s] = h.xv[k].z; v[2 * s + 1] = h.xv[k].w; }
+    if (C) { C[4 * s] = h.C[k].x; C[4 * s + 1] = h.C[k].y; C[4 * s + 2] = h.C[k].z; C[4 * s + 3] = h.C[k].w; }
+    if (F) { F[4 * s] = h.F[k].x; F[4 * s + 1] = h.F[k].y; F[4 * s + 2] = h.F[k].z; F[4 * s + 3] = h.F[k].w; }
+    if (material) material[s] = h.mat[k];
+    if (Jp) Jp[s] = h.Jp[k];
+    if (glow) glow[s] = h.glow[k];
+    if (fiber) { fiber[2 * s] = h.fiber[k].x; fiber[2 * s + 1] = h.fiber[k].y; }
+  }
+  return JF_OK;
+}
+
+int jf_write_particles(jf_engine* e, int32_t m, const float* x, const float* v, const float* C, const float* F,
+                       const float* Jp, const float* glow) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  int rc = set_device(e);
+  if (rc) return rc;
+  HostInstance h;
+  if ((rc = download_instance(e, m, h))) return rc;
+  const size_t n = h.slot.size();
+  for (size_t k = 0; k < n; ++k) {
+    const size_t s = (size_t)h.slot[k];
+    if (x) { h.xv[k].x = x[2 * s]; h.xv[k].y = x[2 * s + 1]; }
+    if (v) { h.xv[k].z = v[2 * s]; h.xv[k].w = v[2 * s + 1]; }
+    if (C) h.C[k] = make_float4(C[4 * s], C[4 * s + 1], C[4 * s + 2], C[4 * s + 3]);
+    if (F) h.F[k] = make_float4(F[4 * s], F[4 * s + 1], F[4 * s + 2], F[4 * s + 3]);
+    if (Jp) h.Jp[k] = Jp[s];
+    if (glow) h.glow[k] = glow[s];
+  }
+  if ((rc = upload_instance(e, m, h))) return rc;
+  if (x) e->sorted = false;
+  return JF_OK;
+}
+
+int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const JfInst& I = e->inst[m];
+  std::vector<float4> g((size_t)I.nx * I.ny);
+  JF_CK(cudaMemcpyAsync(g.data(), e->d_grid + I.g_off, sizeof(float4) * g.size(), cudaMemcpyDeviceToHost,
+                        e->stream),
+        "read grid");
+  JF_CK(cudaStreamSynchronize(e->stream), "read grid sync");
+  for (int j = 0; j < I.ny; ++j) {
+    for (int i = 0; i < I.nx; ++i) {
+      const float4 q = g[(size_t)j * I.nx + i];
+      const size_t r = (size_t)i * I.ny + j;  // reference layout [nx][ny]
+      if (grid_v) { grid_v[2 * r] = q.x; grid_v[2 * r + 1] = q.y; }
+      if (grid_m) grid_m[r] = q.z;
+    }
+  }
+  return JF_OK;
+}
+
+int jf_error_flags(jf_engine* e, int32_t* out) {
+  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(cudaMemcpyAsync(out, e->d_err, sizeof(int32_t) * e->M, cudaMemcpyDeviceToHost, e->stream), "read flags");
+  JF_CK(cudaStreamSynchronize(e->stream), "flags sync");
+  return JF_OK;
+}
+
+int jf_clear_error_flags(jf_engine* e) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(cudaMemsetAsync(e->d_err, 0, sizeof(int32_t) * e->M, e->stream), "clear flags");
+  return JF_OK;
+}
+
+int64_t jf_kernel_launches(const jf_engine* e) { return e ? e->launches : -1; }
+
+int jf_set_kernel_timing(jf_engine* e, int32_t enable) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(cudaStreamSynchronize(e->stream), "timing sync");
+  collect_timing(e);
+  e->step_ms = e->sort_ms = 0.0;
+  e->step_launches = e->sort_launches = 0;
+  e->timing = enable != 0;
+  return JF_OK;
+}
+
+int jf_kernel_timing(jf_engine* e, double* step_ms, int64_t* step_launches, double* sort_ms,
+                     int64_t* sort_launches) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(cudaStreamSynchronize(e->stream), "timing sync");
+  JF_CK(collect_timing(e), "event elapsed time");
+  if (step_ms) *step_ms = e->step_ms;
+  if (step_launches) *step_launches = e->step_launches;
+  if (sort_ms) *sort_ms = e->sort_ms;
+  if (sort_launches) *sort_launches = e->sort_launches;
+  return JF_OK;
+}
+
+}  // extern "C"

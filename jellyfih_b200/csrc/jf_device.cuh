@@ -1,0 +1,302 @@
+// Device math of the 2-D MLS-MPM substep, shared by the plain and batched
+// paths.  Each function follows the reference engine mpm_sim.py (line numbers
+// cited per function) in its operation order; FP32 throughout, with FMA
+// contraction left to the compiler except in the waveform phase, which is
+// rounded step by step so that the 1 -> 0 drop of the activation lands on the
+// same substep as in the reference.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+// Static per-instance description, built on the host.  FP32 constants are the
+// reference's Python-double expressions rounded once (mpm_sim.py:18-58).
+struct JfInst {
+  int32_t nx, ny;       // grid nodes along x and y (n_grid, n_grid_y)
+  int32_t dcx, dcy;     // damping band widths n_grid // 20, n_grid_y // 20 (:283-284)
+  int32_t band_h;       // grid rows per CTA band (batched path)
+  int32_t n_slots;      // particle slots of this instance
+  int64_t p_off;        // first particle slot in the engine arrays
+  int64_t g_off;        // first grid node in the engine grid array
+  float inv_dx, dx, dt, p_mass;
+  float stress_scale;   // -dt * p_vol * 4 * inv_dx^2 (:250)
+  float c4;             // 4 * inv_dx (:326)
+  float dtg;            // dt * gravity (:329)
+  float y_hi;           // domain_height - 0.001 (:333)
+};
+
+// Mutable per-instance waveform / material parameters (mpm_sim.py:116-149).
+struct JfParams {
+  float actuation;        // instance_actuation
+  float contraction;      // instance_act_contraction
+  float freq;             // instance_freq
+  float payload_density;  // instance_payload_density
+};
+
+// Lame parameters by material id: 0 water, 1 jelly, 2 payload, 3 muscle,
+// anything else the E_base / nu_base default (mpm_sim.py:192-203).
+struct JfMaterials {
+  float mu[5];
+  float la[5];
+};
+
+__device__ __forceinline__ int jf_mat_slot(int mt) { return (mt >= 0 && mt <= 3) ? mt : 4; }
+
+// Activation of the 2-phase waveform (mpm_sim.py:173-180): Python float
+// modulo as a - b*floor(a/b), half-cosine arch while phase < contraction.
+// cos is taken in double and rounded once.
+__host__ __device__ inline float jf_activation(float freq, float contraction, float t) {
+#ifdef __CUDA_ARCH__
+  float period = __fdiv_rn(1.0f, __fmul_rn(1.0f, freq));
+  float q = floorf(__fdiv_rn(t, period));
+  float r = __fsub_rn(t, __fmul_rn(period, q));
+  float phase = __fdiv_rn(r, period);
+  float a = 0.0f;
+  if (phase < contraction) {
+    float arg = __fmul_rn(__fdiv_rn(phase, contraction), 3.14159265f);
+    a = __fmul_rn(0.5f, __fsub_rn(1.0f, (float)cos((double)arg)));
+  }
+  return a;
+#else
+  volatile float period = 1.0f / (1.0f * freq);
+  volatile float q = floorf(t / period);
+  volatile float pq = period * q;
+  volatile float r = t - pq;
+  volatile float phase = r / period;
+  float a = 0.0f;
+  if (phase < contraction) {
+    volatile float ratio = phase / contraction;
+    volatile float arg = ratio * 3.14159265f;
+    volatile float cs = (float)cos((double)arg);
+    volatile float om = 1.0f - cs;
+    a = 0.5f * om;
+  }
+  return a;
+#endif
+}
+
+// 2x2 SVD as taichi 1.7.4 ti.svd computes it (_svd2d): polar decomposition
+// A = R S with R = [[c,-s],[s,c]] from (A00 + A11, A10 - A01), one Jacobi
+// rotation of S unless |S01| < 1e-5, singular values ordered s1 >= s2 with
+// the matching V, U = R V.  Matrices row-major in float4 (00, 01, 10, 11).
+__device__ __forceinline__ void jf_svd2(float4 A, float4& U, float2& sig, float4& V) {
+  float x = A.x + A.w;
+  float y = A.z - A.y;
+  float scale = 1.0f / sqrtf(x * x + y * y);
+  float c = x * scale;
+  float s = y * scale;
+  float ms = -s;
+  float S00 = c * A.x + s * A.z;
+  float S01 = c * A.y + s * A.w;
+  float S11 = ms * A.y + c * A.w;
+  float cc, ss, s1, s2;
+  if (fabsf(S01) < 1e-5f) {
+    cc = 1.0f; ss = 0.0f;
+    s1 = S00; s2 = S11;
+  } else {
+    float tao = 0.5f * (S00 - S11);
+    float w = sqrtf(tao * tao + S01 * S01);
+    float t = tao > 0.0f ? S01 / (tao + w) : S01 / (tao - w);
+    cc = 1.0f / sqrtf(t * t + 1.0f);
+    ss = (-t) * cc;
+    s1 = (cc * cc * S00 - 2.0f * cc * ss * S01) + ss * ss * S11;
+    s2 = (ss * ss * S00 + 2.0f * cc * ss * S01) + cc * cc * S11;
+  }
+  float V00, V01, V10, V11;
+  if (s1 < s2) {
+    float tmp = s1; s1 = s2; s2 = tmp;
+    V00 = -ss; V01 = cc; V10 = -cc; V11 = -ss;
+  } else {
+    V00 = cc; V01 = ss; V10 = -ss; V11 = cc;
+  }
+  U = make_float4(c * V00 + ms * V10, c * V01 + ms * V11, s * V00 + c * V10, s * V01 + c * V11);
+  V = make_float4(V00, V01, V10, V11);
+  sig = make_float2(s1, s2);
+}
+
+// Quadratic B-spline stencil of one particle (mpm_sim.py:183-187).  Returns
+// false when the particle lies outside [0, n-2) in either axis; the cast
+// truncates toward zero, as Taichi's .cast(int) does.
+struct JfStencil {
+  int bx, by;
+  float fx0, fx1;
+  float wx0, wx1, wx2, wy0, wy1, wy2;
+};
+
+__device__ __forceinline__ bool jf_stencil(const JfInst& I, float2 x, JfStencil& st) {
+  st.bx = (int)(x.x * I.inv_dx - 0.5f);
+  st.by = (int)(x.y * I.inv_dx - 0.5f);
+  if (st.bx < 0 || st.by < 0 || st.bx >= I.nx - 2 || st.by >= I.ny - 2) return false;
+  st.fx0 = x.x * I.inv_dx - (float)st.bx;
+  st.fx1 = x.y * I.inv_dx - (float)st.by;
+  float a0 = 1.5f - st.fx0, a1 = 1.5f - st.fx1;
+  float b0 = st.fx0 - 1.0f, b1 = st.fx1 - 1.0f;
+  float e0 = st.fx0 - 0.5f, e1 = st.fx1 - 0.5f;
+  st.wx0 = 0.5f * (a0 * a0); st.wx1 = 0.75f - b0 * b0; st.wx2 = 0.5f * (e0 * e0);
+  st.wy0 = 0.5f * (a1 * a1); st.wy1 = 0.75f - b1 * b1; st.wy2 = 0.5f * (e1 * e1);
+  return true;
+}
+
+__device__ __forceinline__ float jf_w(const JfStencil& s, int axis, int k) {
+  if (axis == 0) return k == 0 ? s.wx0 : (k == 1 ? s.wx1 : s.wx2);
+  return k == 0 ? s.wy0 : (k == 1 ? s.wy1 : s.wy2);
+}
+
+// Per-particle scatter terms of P2G: mass, APIC affine matrix and momentum.
+struct JfScatter {
+  float mass;
+  float af00, af01, af10, af11;
+  float mv0, mv1;
+};
+
+// P2G for one particle (mpm_sim.py:189-254): F <- (I + dt C) F, SVD,
+// plasticity (payload clamps sigma to [1-5e-3, 1+5e-3]; water resets
+// F = sqrt(J) I), fixed-corotated Kirchhoff stress plus the muscle's active
+// fibre stress, scaled, plus the APIC term.  Jp is updated only when the
+// material is payload (for every other material the ratio is exactly 1).
+__device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMaterials& mats, int mt,
+                                                float2 v, float4 C, float4& F, float& Jp,
+                                                float2 fiber, float pressure, float pdens,
+                                                JfScatter& o) {
+  const float dt = I.dt;
+  {
+    float A00 = 1.0f + dt * C.x, A01 = dt * C.y, A10 = dt * C.z, A11 = 1.0f + dt * C.w;
+    float F00 = A00 * F.x + A01 * F.z;
+    float F01 = A00 * F.y + A01 * F.w;
+    float F10 = A10 * F.x + A11 * F.z;
+    float F11 = A10 * F.y + A11 * F.w;
+    F = make_float4(F00, F01, F10, F11);
+  }
+  // constant-index selects keep the table in registers (no local-memory copy)
+  const int ms = jf_mat_slot(mt);
+  const float mu = ms == 0 ? mats.mu[0] : ms == 1 ? mats.mu[1] : ms == 2 ? mats.mu[2]
+                 : ms == 3 ? mats.mu[3] : mats.mu[4];
+  const float la = ms == 0 ? mats.la[0] : ms == 1 ? mats.la[1] : ms == 2 ? mats.la[2]
+                 : ms == 3 ? mats.la[3] : mats.la[4];
+  float mass = I.p_mass;
+  if (mt == 2) mass = mass * pdens;
+
+  float4 U, V;
+  float2 sig;
+  jf_svd2(F, U, sig, V);
+  sig.x = fmaxf(sig.x, 1e-6f);
+  sig.y = fmaxf(sig.y, 1e-6f);
+  float J;
+  if (mt == 2) {
+    float n0 = fminf(fmaxf(sig.x, 0.995f), 1.005f);
+    float n1 = fminf(fmaxf(sig.y, 0.995f), 1.005f);
+    Jp = Jp * (sig.x / n0);
+    Jp = Jp * (sig.y / n1);
+    sig = make_float2(n0, n1);
+  }
+  J = sig.x * sig.y;
+  if (mt == 0) {
+    float sj = sqrtf(J);
+    F = make_float4(sj, 0.0f, 0.0f, sj);
+  } else if (mt == 2) {
+    float US00 = U.x * sig.x, US01 = U.y * sig.y, US10 = U.z * sig.x, US11 = U.w * sig.y;
+    F = make_float4(US00 * V.x + US01 * V.y, US00 * V.z + US01 * V.w,
+                    US10 * V.x + US11 * V.y, US10 * V.z + US11 * V.w);
+  }
+  float R00 = U.x * V.x + U.y * V.y;
+  float R01 = U.x * V.z + U.y * V.w;
+  float R10 = U.z * V.x + U.w * V.y;
+  float R11 = U.z * V.z + U.w * V.w;
+  float twomu = 2.0f * mu;
+  float E00 = twomu * (F.x - R00), E01 = twomu * (F.y - R01);
+  float E10 = twomu * (F.z - R10), E11 = twomu * (F.w - R11);
+  float diag = la * J * (J - 1.0f);
+  float s00 = (E00 * F.x + E01 * F.y) + diag;
+  float s01 = E00 * F.z + E01 * F.w;
+  float s10 = E10 * F.x + E11 * F.y;
+  float s11 = (E10 * F.z + E11 * F.w) + diag;
+  if (mt == 3) {
+    s00 = s00 + fiber.x * fiber.x * pressure * J;
+    s01 = s01 + fiber.x * fiber.y * pressure * J;
+    s10 = s10 + fiber.y * fiber.x * pressure * J;
+    s11 = s11 + fiber.y * fiber.y * pressure * J;
+  }
+  const float k = I.stress_scale;
+  o.mass = mass;
+  o.af00 = k * s00 + mass * C.x;
+  o.af01 = k * s01 + mass * C.y;
+  o.af10 = k * s10 + mass * C.z;
+  o.af11 = k * s11 + mass * C.w;
+  o.mv0 = mass * v.x;
+  o.mv1 = mass * v.y;
+}
+
+// Contribution of a particle to stencil node (i, j), i, j in 0..2
+// (mpm_sim.py:256-271): (weight * momentum_x, weight * momentum_y, weight * mass).
+__device__ __forceinline__ float3 jf_node_contrib(const JfInst& I, const JfStencil& st,
+                                                  const JfScatter& sc, int i, int j) {
+  float d0 = ((float)i - st.fx0) * I.dx;
+  float d1 = ((float)j - st.fx1) * I.dx;
+  float weight = jf_w(st, 0, i) * jf_w(st, 1, j);
+  float c0 = weight * (sc.mv0 + (sc.af00 * d0 + sc.af01 * d1));
+  float c1 = weight * (sc.mv1 + (sc.af10 * d0 + sc.af11 * d1));
+  return make_float3(c0, c1, weight * sc.mass);
+}
+
+// Grid node update (mpm_sim.py:274-309): normalise by mass, damp in a band of
+// n//20 nodes on all four sides, zero the velocity component pointing into a
+// wall within 3 nodes.  Nodes without mass keep their (zero) momentum.
+__device__ __forceinline__ float2 jf_grid_node(const JfInst& I, int i, int j, float gx, float gy,
+                                               float m) {
+  if (!(m > 0.0f)) return make_float2(gx, gy);
+  float g0 = gx / m, g1 = gy / m;
+  float damp = 1.0f;
+  if (i < I.dcx) damp = damp * (0.95f + 0.05f * (float)i / (float)I.dcx);
+  if (i > I.nx - I.dcx) damp = damp * (0.95f + 0.05f * (float)(I.nx - i) / (float)I.dcx);
+  if (j < I.dcy) damp = damp * (0.95f + 0.05f * (float)j / (float)I.dcy);
+  if (j > I.ny - I.dcy) damp = damp * (0.95f + 0.05f * (float)(I.ny - j) / (float)I.dcy);
+  g0 = g0 * damp;
+  g1 = g1 * damp;
+  if (i < 3 && g0 < 0.0f) g0 = 0.0f;
+  if (i > I.nx - 3 && g0 > 0.0f) g0 = 0.0f;
+  if (j < 3 && g1 < 0.0f) g1 = 0.0f;
+  if (j > I.ny - 3 && g1 > 0.0f) g1 = 0.0f;
+  return make_float2(g0, g1);
+}
+
+// G2P for one particle (mpm_sim.py:315-333): APIC gather of v and C from the
+// updated grid when the stencil is in range, then gravity, advection and the
+// wall clamp for every live particle.  `gather(i_node, j_node)` returns the
+// updated grid velocity of a node.
+template <class Gather>
+__device__ __forceinline__ void jf_g2p_particle(const JfInst& I, float2& x, float2& v, float4& C,
+                                                Gather gather) {
+  JfStencil st;
+  if (jf_stencil(I, x, st)) {
+    float nv0 = 0.f, nv1 = 0.f, c00 = 0.f, c01 = 0.f, c10 = 0.f, c11 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        float d0 = (float)i - st.fx0, d1 = (float)j - st.fx1;
+        float2 g = gather(st.bx + i, st.by + j);
+        float weight = jf_w(st, 0, i) * jf_w(st, 1, j);
+        nv0 = nv0 + weight * g.x;
+        nv1 = nv1 + weight * g.y;
+        float k = I.c4 * weight;
+        c00 = c00 + k * (g.x * d0);
+        c01 = c01 + k * (g.x * d1);
+        c10 = c10 + k * (g.y * d0);
+        c11 = c11 + k * (g.y * d1);
+      }
+    }
+    v = make_float2(nv0, nv1);
+    C = make_float4(c00, c01, c10, c11);
+  }
+  v.y = v.y - I.dtg;
+  // rounded as the reference rounds it (product, then sum): a fused
+  // multiply-add here shifts 1,000-step payload displacement by ~0.2%
+  x.x = __fadd_rn(x.x, __fmul_rn(I.dt, v.x));
+  x.y = __fadd_rn(x.y, __fmul_rn(I.dt, v.y));
+  x.x = fmaxf(fminf(x.x, 0.999f), 0.001f);
+  x.y = fmaxf(fminf(x.y, I.y_hi), 0.001f);
+}
+
+// visual_glow decay (mpm_sim.py:336-338), render-only.
+__device__ __forceinline__ float jf_glow(float glow, float Jp) {
+  return fmaxf(glow * 0.9f, fabsf(1.0f - Jp));
+}

@@ -1,0 +1,101 @@
+// Internal engine state shared by the C-ABI entry points and the two step
+// paths (plain per-instance launches, batched persistent cluster launch).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/jellyfih.h"
+#include "jf_device.cuh"
+
+// Particle arrays in engine order.  The plain path keeps slot order; the
+// batched path keeps every instance's live particles sorted by grid cell, and
+// slot[k] maps engine position k back to the caller's slot index.
+struct JfParticles {
+  float4* xv = nullptr;     // (x0, x1, v0, v1)
+  float4* C = nullptr;      // APIC affine velocity, row-major
+  float4* F = nullptr;      // deformation gradient, row-major
+  int32_t* mat = nullptr;   // material id, -1 = dead slot
+  float2* fiber = nullptr;  // muscle fibre direction
+  float* Jp = nullptr;      // plastic volume ratio
+  float* glow = nullptr;    // render-only glow
+  int32_t* slot = nullptr;  // engine position -> slot index
+};
+
+struct jf_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int32_t M = 0;
+  double dt = 2e-5;
+  int32_t path = JF_PATH_PLAIN;
+  uint32_t flags = 0;
+  int32_t resort_interval = 16;
+  int32_t block_threads = 512;
+  int32_t cluster = 4;
+
+  std::vector<JfInst> inst;        // host copy
+  std::vector<JfParams> params;    // host mirror (authoritative)
+  bool params_dirty = true;
+  int64_t total_slots = 0;
+  int64_t total_nodes = 0;
+  int32_t max_slots = 0;
+  int32_t max_cells = 0;           // max nx * ny
+  int32_t win_nodes = 0;           // max (band_h + halo rows) * nx, batched smem window
+
+  JfInst* d_inst = nullptr;
+  JfParams* d_params = nullptr;
+  JfParticles p;                   // live buffers
+  JfParticles q;                   // batched path: sort destination
+  int32_t* d_keys = nullptr;       // batched path: cell key per engine position
+  int32_t* d_counts = nullptr;     // batched path: M x (max_cells + 2) histogram / cursors
+  int32_t* d_band = nullptr;       // batched path: M x (cluster + 1) particle ranges
+  float4* d_grid = nullptr;        // grid nodes (node = g_off + j * nx + i): (v0, v1, m, 0)
+  double* d_stats = nullptr;       // M x 6 CoM sums (payload y, count, x; body y, count, x)
+  int32_t* d_err = nullptr;        // per-instance non-finite flags
+  float* d_stage = nullptr;        // host <-> device staging (max_slots * 8 floats)
+  int32_t* d_stage_i = nullptr;    // staging for ints (max_slots * 2)
+
+  bool sorted = false;             // batched path: particle order valid for the current state
+  float t = 0.0f;                  // sim_time (FP32 running sum, mpm_sim.py:340)
+  int64_t launches = 0;            // kernels launched by this engine
+  std::string err;
+
+  // optional device timing of step and sort kernels
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> step_events, sort_events;
+  std::vector<cudaEvent_t> event_pool;
+  double step_ms = 0.0, sort_ms = 0.0;
+  int64_t step_launches = 0, sort_launches = 0;
+};
+
+// Event pair bracketing one timed region (no-op when timing is off).
+struct JfTimed {
+  jf_engine* e;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* list;
+  cudaEvent_t a = nullptr, b = nullptr;
+  JfTimed(jf_engine* eng, bool sort);
+  ~JfTimed();
+};
+
+// Lame parameters by material id (mpm_sim.py:25-48), passed to kernels by value.
+JfMaterials jf_materials();
+
+// Plain path: instance-by-instance launches of clear / P2G / grid update / G2P.
+cudaError_t jf_plain_step(jf_engine* e, int64_t n_steps);
+
+// Batched path: re-sort plus one persistent cluster launch per chunk.
+cudaError_t jf_batched_step(jf_engine* e, int64_t n_steps);
+cudaError_t jf_batched_sort(jf_engine* e);
+size_t jf_batched_smem_bytes(const jf_engine* e);
+
+// CoM sums of every instance into e->d_stats (M x 6 doubles).
+cudaError_t jf_stats_launch(jf_engine* e);
+
+// Kernels used by the C-ABI for loading, reading and writing particles.
+cudaError_t jf_load_launch(jf_engine* e, int m, int32_t n);
+// Copies instance m's glow into slot order at d_stage + 4 * max_slots.
+cudaError_t jf_glow_to_slot_order(jf_engine* e, int m);

@@ -1,0 +1,230 @@
+// Plain path: one instance per launch sequence, structured like the
+// reference's substep() offloads (mpm_sim.py:160-340): grid clear, P2G with
+// global atomics, grid update, G2P.  Also the CoM reduction and the
+// load / glow-reorder kernels shared with the batched path.
+#include "jf_engine.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+JfMaterials host_materials() {
+  // mpm_sim.py:25-48, Python doubles rounded once.
+  const double E_base = 0.1e4, nu_base = 0.2, E_jelly = 0.7e3, nu_jelly = 0.3;
+  const double E_pay = 2.0e5, nu_pay = 0.2, water_lambda = 100000.0;
+  const float mu0 = (float)(E_base / (2 * (1 + nu_base)));
+  const float la0 = (float)(E_base * nu_base / ((1 + nu_base) * (1 - 2 * nu_base)));
+  const float muj = (float)(E_jelly / (2 * (1 + nu_jelly)));
+  const float laj = (float)(E_jelly * nu_jelly / ((1 + nu_jelly) * (1 - 2 * nu_jelly)));
+  const float mup = (float)(E_pay / (2 * (1 + nu_pay)));
+  const float lap = (float)(E_pay * nu_pay / ((1 + nu_pay) * (1 - 2 * nu_pay)));
+  JfMaterials m;
+  m.mu[0] = 0.0f; m.la[0] = (float)water_lambda;  // water
+  m.mu[1] = muj;  m.la[1] = laj;                  // jelly
+  m.mu[2] = mup;  m.la[2] = lap;                  // payload
+  m.mu[3] = muj;  m.la[3] = laj;                  // muscle
+  m.mu[4] = mu0;  m.la[4] = la0;                  // any other id
+  return m;
+}
+
+__global__ void plain_p2g(JfInst I, JfMaterials mats, JfParams P, float pressure,
+                          const float4* __restrict__ xv, const float4* __restrict__ Cm,
+                          float4* __restrict__ Fm, const int32_t* __restrict__ mat,
+                          float* __restrict__ Jp, const float2* __restrict__ fiber,
+                          float4* __restrict__ grid) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  const int mt = mat[g];
+  if (mt < 0) return;
+  const float4 a = xv[g];
+  const float2 x = make_float2(a.x, a.y), v = make_float2(a.z, a.w);
+  JfStencil st;
+  if (!jf_stencil(I, x, st)) return;
+  float4 F = Fm[g];
+  const float4 C = Cm[g];
+  float jp = (mt == 2) ? Jp[g] : 1.0f;
+  const float2 fb = (mt == 3) ? fiber[g] : make_float2(0.0f, 1.0f);
+  JfScatter sc;
+  jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
+  Fm[g] = F;
+  if (mt == 2) Jp[g] = jp;
+  float4* gi = grid + I.g_off;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float3 c = jf_node_contrib(I, st, sc, i, j);
+      atomicAdd(gi + (int64_t)(st.by + j) * I.nx + (st.bx + i), make_float4(c.x, c.y, c.z, 0.0f));
+    }
+  }
+}
+
+__global__ void plain_grid(JfInst I, float4* __restrict__ grid) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= I.nx * I.ny) return;
+  const int i = n % I.nx, j = n / I.nx;
+  const float4 g = grid[I.g_off + n];
+  const float2 u = jf_grid_node(I, i, j, g.x, g.y, g.z);
+  grid[I.g_off + n] = make_float4(u.x, u.y, g.z, 0.0f);
+}
+
+__global__ void plain_g2p(JfInst I, int m, float4* __restrict__ xv, float4* __restrict__ Cm,
+                          const int32_t* __restrict__ mat, const float* __restrict__ Jp,
+                          float* __restrict__ glow, const float4* __restrict__ grid,
+                          int32_t* __restrict__ err, int do_glow) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  if (do_glow) glow[g] = jf_glow(glow[g], Jp[g]);
+  if (mat[g] < 0) return;
+  const float4 a = xv[g];
+  float2 x = make_float2(a.x, a.y), v = make_float2(a.z, a.w);
+  float4 C = Cm[g];
+  const float4* gi = grid + I.g_off;
+  const int nx = I.nx;
+  jf_g2p_particle(I, x, v, C, [&](int ni, int nj) {
+    const float4 q = gi[(int64_t)nj * nx + ni];
+    return make_float2(q.x, q.y);
+  });
+  if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(err + m, 1);
+  xv[g] = make_float4(x.x, x.y, v.x, v.y);
+  Cm[g] = C;
+}
+
+__global__ void stats_kernel(const JfInst* __restrict__ inst, const float4* __restrict__ xv,
+                             const int32_t* __restrict__ mat, double* __restrict__ out) {
+  const int m = blockIdx.y;
+  const JfInst I = inst[m];
+  double py = 0, pc = 0, px = 0, by = 0, bc = 0, bx = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < I.n_slots; k += gridDim.x * blockDim.x) {
+    const int64_t g = I.p_off + k;
+    const int mt = mat[g];
+    if (mt == 2) {
+      const float4 a = xv[g];
+      py += (double)a.y; pc += 1.0; px += (double)a.x;
+    } else if (mt == 1 || mt == 3) {
+      const float4 a = xv[g];
+      by += (double)a.y; bc += 1.0; bx += (double)a.x;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    py += __shfl_down_sync(0xffffffffu, py, off);
+    pc += __shfl_down_sync(0xffffffffu, pc, off);
+    px += __shfl_down_sync(0xffffffffu, px, off);
+    by += __shfl_down_sync(0xffffffffu, by, off);
+    bc += __shfl_down_sync(0xffffffffu, bc, off);
+    bx += __shfl_down_sync(0xffffffffu, bx, off);
+  }
+  if ((threadIdx.x & 31) == 0 && (pc > 0 || bc > 0)) {
+    double* o = out + 6 * m;
+    atomicAdd(o + 0, py); atomicAdd(o + 1, pc); atomicAdd(o + 2, px);
+    atomicAdd(o + 3, by); atomicAdd(o + 4, bc); atomicAdd(o + 5, bx);
+  }
+}
+
+// Reset one instance from staged host arrays (mpm_sim.py:715-727).
+__global__ void load_kernel(JfInst I, int32_t n, const float* __restrict__ pos,
+                            const int32_t* __restrict__ mt_in, const float* __restrict__ fib,
+                            int has_fiber, JfParticles p, const float* __restrict__ glow_slot) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  float2 x = make_float2(-1.0f, -1.0f);
+  int mt = -1;
+  float2 fb = make_float2(0.0f, 1.0f);
+  if (k < n) {
+    x = make_float2(pos[2 * k], pos[2 * k + 1]);
+    mt = mt_in[k];
+    if (has_fiber) fb = make_float2(fib[2 * k], fib[2 * k + 1]);
+  }
+  p.xv[g] = make_float4(x.x, x.y, 0.0f, 0.0f);
+  p.C[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  p.F[g] = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
+  p.mat[g] = mt;
+  p.fiber[g] = fb;
+  p.Jp[g] = 1.0f;
+  p.glow[g] = glow_slot[k];
+  p.slot[g] = k;
+}
+
+__global__ void glow_to_slot_kernel(JfInst I, const float* __restrict__ glow,
+                                    const int32_t* __restrict__ slot, float* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  out[slot[g]] = glow[g];
+}
+
+inline int blocks_for(int64_t n) { return (int)((n + kThreads - 1) / kThreads); }
+
+}  // namespace
+
+JfMaterials jf_materials() { return host_materials(); }
+
+cudaError_t jf_plain_step(jf_engine* e, int64_t n_steps) {
+  const JfMaterials mats = host_materials();
+  const float dtf = (float)e->dt;
+  const int do_glow = (e->flags & JF_FLAG_GLOW) ? 1 : 0;
+  float t_end = e->t;
+  for (int m = 0; m < e->M; ++m) {
+    const JfInst& I = e->inst[m];
+    const JfParams P = e->params[m];
+    const int nodes = I.nx * I.ny;
+    float t = e->t;
+    for (int64_t s = 0; s < n_steps; ++s) {
+      const float pressure = P.actuation * jf_activation(P.freq, P.contraction, t);
+      JfTimed timed(e, false);
+      cudaError_t err = cudaMemsetAsync(e->d_grid + I.g_off, 0, sizeof(float4) * nodes, e->stream);
+      if (err != cudaSuccess) return err;
+      if (I.n_slots > 0) {
+        plain_p2g<<<blocks_for(I.n_slots), kThreads, 0, e->stream>>>(
+            I, mats, P, pressure, e->p.xv, e->p.C, e->p.F, e->p.mat, e->p.Jp, e->p.fiber, e->d_grid);
+      }
+      plain_grid<<<blocks_for(nodes), kThreads, 0, e->stream>>>(I, e->d_grid);
+      if (I.n_slots > 0) {
+        plain_g2p<<<blocks_for(I.n_slots), kThreads, 0, e->stream>>>(
+            I, m, e->p.xv, e->p.C, e->p.mat, e->p.Jp, e->p.glow, e->d_grid, e->d_err, do_glow);
+      }
+      e->launches += (I.n_slots > 0) ? 3 : 1;
+      t = t + dtf;
+    }
+    t_end = t;
+  }
+  e->t = t_end;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_stats_launch(jf_engine* e) {
+  cudaError_t err = cudaMemsetAsync(e->d_stats, 0, sizeof(double) * 6 * e->M, e->stream);
+  if (err != cudaSuccess) return err;
+  int blocks = blocks_for(e->max_slots);
+  if (blocks > 64) blocks = 64;
+  if (blocks < 1) blocks = 1;
+  stats_kernel<<<dim3(blocks, e->M), kThreads, 0, e->stream>>>(e->d_inst, e->p.xv, e->p.mat,
+                                                                 e->d_stats);
+  e->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_glow_to_slot_order(jf_engine* e, int m) {
+  const JfInst& I = e->inst[m];
+  if (I.n_slots == 0) return cudaSuccess;
+  glow_to_slot_kernel<<<blocks_for(I.n_slots), kThreads, 0, e->stream>>>(
+      I, e->p.glow, e->p.slot, e->d_stage + 4 * (int64_t)e->max_slots);
+  e->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_load_launch(jf_engine* e, int m, int32_t n) {
+  // staging layout: d_stage[0 .. 2S) pos, [2S .. 4S) fibre, [4S .. 5S) glow in slot
+  // order; d_stage_i[0 .. S) material.
+  const JfInst& I = e->inst[m];
+  if (I.n_slots == 0) return cudaSuccess;
+  const int64_t S = e->max_slots;
+  load_kernel<<<blocks_for(I.n_slots), kThreads, 0, e->stream>>>(
+      I, n, e->d_stage, e->d_stage_i, e->d_stage + 2 * S, 1, e->p, e->d_stage + 4 * S);
+  e->launches += 1;
+  return cudaGetLastError();
+}

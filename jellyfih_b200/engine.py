@@ -1,0 +1,198 @@
+"""Python host of the engine: one :class:`Engine` owns one libjellyfih handle.
+
+Arrays passed in and returned use the reference's field layouts
+(mpm_sim.py:86-93): positions / velocities / fibres (n, 2), C and F (n, 2, 2)
+row-major, material (n,) int32, grids (nx, ny, 2) and (nx, ny).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+DT = 2e-5  # mpm_sim.py:19
+
+
+@dataclass(frozen=True)
+class InstanceSpec:
+    """Slots and grid of one instance (mpm_sim.py:11-16)."""
+    n_slots: int = 80000
+    n_grid: int = 128
+    n_grid_y: int = 128
+    domain_height: float = 1.0
+
+
+def _f32(a, shape=None):
+    arr = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and arr.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {arr.shape}")
+    return arr
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Engine:
+    """A batch of independent MLS-MPM instances on one GPU.
+
+    ``path='batched'`` advances every instance in one persistent cluster launch
+    per chunk; ``path='plain'`` launches clear / P2G / grid update / G2P per
+    instance and substep, as the reference's substep() offloads do.
+    """
+
+    def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
+                 glow: bool = False, device: int = 0, resort_interval: int = 16,
+                 block_threads: int = 512):
+        self._lib = L.load()
+        self.instances = list(instances)
+        self.M = len(self.instances)
+        self.path = path
+        descs = (L.JfInstanceDesc * self.M)(*[
+            L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
+        cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
+                         L.JF_FLAG_GLOW if glow else 0, device, resort_interval, block_threads)
+        h = L._E()
+        rc = self._lib.jf_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != L.JF_OK:
+            raise L.JfError(rc, self._lib.jf_last_error(None).decode())
+        self._h = h
+        self.dt = dt
+
+    # -- plumbing --------------------------------------------------------
+    def _check(self, rc):
+        if rc != L.JF_OK:
+            raise L.JfError(rc, self._lib.jf_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.jf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._lib.jf_kernel_launches(self._h))
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        """Bracket step / sort kernels with CUDA events (resets the totals)."""
+        self._check(self._lib.jf_set_kernel_timing(self._h, 1 if enable else 0))
+
+    def kernel_timing(self) -> dict:
+        """Summed device time (ms) and launches of step and re-sort kernels."""
+        sm, sl, om, ol = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_int64()
+        self._check(self._lib.jf_kernel_timing(self._h, ctypes.byref(sm), ctypes.byref(sl),
+                                               ctypes.byref(om), ctypes.byref(ol)))
+        return {"step_ms": sm.value, "step_launches": sl.value, "sort_ms": om.value,
+                "sort_launches": ol.value}
+
+    def set_stream(self, stream) -> None:
+        """Queue work on ``stream`` (a cudaStream_t as int, or a torch.cuda.Stream)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        self._check(self._lib.jf_set_stream(self._h, handle))
+
+    # -- state -------------------------------------------------------------
+    def load(self, m: int, pos, material, fiber=None) -> None:
+        """load_particles (mpm_sim.py:730-736) for instance ``m``."""
+        n = len(material)
+        pos = _f32(pos, (n, 2))
+        mat = np.ascontiguousarray(material, dtype=np.int32)
+        fib = None if fiber is None else _f32(fiber, (n, 2))
+        self._check(self._lib.jf_load_instance(self._h, m, _ptr(pos), _ptr(mat), _ptr(fib), n))
+
+    def set_params(self, actuation=None, contraction=None, freq=None, payload_density=None) -> None:
+        arrs = [None if a is None else _f32(np.broadcast_to(np.asarray(a, np.float32), (self.M,)))
+                for a in (actuation, contraction, freq, payload_density)]
+        self._check(self._lib.jf_set_params(self._h, *[_ptr(a) for a in arrs]))
+
+    def get_params(self) -> dict:
+        out = {k: np.zeros(self.M, np.float32) for k in ("actuation", "contraction", "freq",
+                                                          "payload_density")}
+        self._check(self._lib.jf_get_params(self._h, *[_ptr(out[k]) for k in (
+            "actuation", "contraction", "freq", "payload_density")]))
+        return out
+
+    @property
+    def time(self) -> np.float32:
+        t = ctypes.c_float()
+        self._check(self._lib.jf_get_time(self._h, ctypes.byref(t)))
+        return np.float32(t.value)
+
+    @time.setter
+    def time(self, t) -> None:
+        self._check(self._lib.jf_set_time(self._h, float(np.float32(t))))
+
+    def step(self, n: int = 1) -> None:
+        self._check(self._lib.jf_step(self._h, int(n)))
+
+    def sync(self) -> None:
+        self._check(self._lib.jf_sync(self._h))
+
+    # -- readback ------------------------------------------------------------
+    def payload_stats(self) -> np.ndarray:
+        out = np.zeros((self.M, 3), np.float64)
+        self._check(self._lib.jf_payload_stats(self._h, _ptr(out)))
+        return out
+
+    def stats_any(self) -> np.ndarray:
+        out = np.zeros((self.M, 3), np.float64)
+        self._check(self._lib.jf_stats_any(self._h, _ptr(out)))
+        return out
+
+    def stats_raw(self) -> np.ndarray:
+        """(M, 6) FP64 sums: payload [sum_y, count, sum_x], body [sum_y, count, sum_x]."""
+        out = np.zeros((self.M, 6), np.float64)
+        self._check(self._lib.jf_stats_raw(self._h, _ptr(out)))
+        return out
+
+    def run_headless(self, steps: int) -> np.ndarray:
+        out = np.zeros((self.M, 5), np.float64)
+        self._check(self._lib.jf_run_headless(self._h, int(steps), _ptr(out)))
+        return out
+
+    def read(self, m: int) -> dict:
+        n = self.instances[m].n_slots
+        d = {"x": np.zeros((n, 2), np.float32), "v": np.zeros((n, 2), np.float32),
+             "C": np.zeros((n, 2, 2), np.float32), "F": np.zeros((n, 2, 2), np.float32),
+             "material": np.zeros(n, np.int32), "Jp": np.zeros(n, np.float32),
+             "glow": np.zeros(n, np.float32), "fiber": np.zeros((n, 2), np.float32)}
+        self._check(self._lib.jf_read_particles(self._h, m, *[_ptr(d[k]) for k in (
+            "x", "v", "C", "F", "material", "Jp", "glow", "fiber")]))
+        return d
+
+    def write(self, m: int, x=None, v=None, C=None, F=None, Jp=None, glow=None) -> None:
+        n = self.instances[m].n_slots
+        args = [None if x is None else _f32(x, (n, 2)), None if v is None else _f32(v, (n, 2)),
+                None if C is None else _f32(C, (n, 2, 2)), None if F is None else _f32(F, (n, 2, 2)),
+                None if Jp is None else _f32(Jp, (n,)), None if glow is None else _f32(glow, (n,))]
+        self._check(self._lib.jf_write_particles(self._h, m, *[_ptr(a) for a in args]))
+
+    def read_grid(self, m: int):
+        s = self.instances[m]
+        gv = np.zeros((s.n_grid, s.n_grid_y, 2), np.float32)
+        gm = np.zeros((s.n_grid, s.n_grid_y), np.float32)
+        self._check(self._lib.jf_read_grid(self._h, m, _ptr(gv), _ptr(gm)))
+        return gv, gm
+
+    def error_flags(self) -> np.ndarray:
+        out = np.zeros(self.M, np.int32)
+        self._check(self._lib.jf_error_flags(self._h, _ptr(out)))
+        return out
+
+    def clear_error_flags(self) -> None:
+        self._check(self._lib.jf_clear_error_flags(self._h))

@@ -1,0 +1,272 @@
+"""GPU parity: libjellyfih.so (plain and batched paths) against the reference.
+
+* Golden fixtures recorded from the reference's own mpm_sim.py (tests/golden)
+  pin single substeps and a few consecutive substeps: every particle field and
+  the grid must agree within 1e-5 relative to the field's max-norm, the
+  difference allowed by a different atomic summation order and FMA
+  contraction.  Positions are compared to within a few FP32 ulps.
+* Longer runs compare against the CPU oracle (oracle/, itself bit-exact to
+  the goldens).  After 1,000 substeps the payload displacement of two FP32
+  runs that differ only in the order of the P2G sums already differs by about
+  0.7% (measured with the oracle itself), so the long-run tolerance is stated
+  against that band rather than 1e-3.
+"""
+import numpy as np
+import pytest
+
+import golden_io as G
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+PATHS = ("plain", "batched")
+FIELD_RTOL = 1e-5
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import build
+    build.build()
+
+
+def _engine(specs, path, **kw):
+    from jellyfih_b200 import Engine
+    return Engine(specs, path=path, **kw)
+
+
+def _spec(d):
+    from jellyfih_b200 import InstanceSpec
+    n = len(d["in0_material"])
+    return InstanceSpec(n, int(d["n_grid"]), int(d["n_grid_y"]), float(d["domain_height"]))
+
+
+def _load_golden(e, d):
+    M = G.n_instances(d)
+    for m in range(M):
+        e.load(m, d[f"in{m}_x"], d[f"in{m}_material"], d[f"in{m}_fiber"])
+        e.write(m, v=d[f"in{m}_v"], C=d[f"in{m}_C"], F=d[f"in{m}_F"], Jp=d[f"in{m}_Jp"],
+                glow=d[f"in{m}_glow"])
+    keys = ("actuation", "contraction", "freq", "payload_density")
+    e.set_params(**{k: d[f"param_{k}"] for k in keys})
+
+
+def assert_norm_close(a, b, rtol, what):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.abs(b).max()
+    err = np.abs(a - b).max()
+    assert err <= rtol * max(scale, 1e-30), f"{what}: max|diff| {err:.3e} > {rtol} * {scale:.3e}"
+
+
+def assert_positions_close(a, b, ulps, what):
+    tol = ulps * np.spacing(np.float32(np.abs(b).max()))
+    err = np.abs(a.astype(np.float64) - b).max()
+    assert err <= tol, f"{what}: max|diff| {err:.3e} > {ulps} ulp ({tol:.3e})"
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("case", G.STEP_CASES)
+def test_substeps_match_reference_goldens(case, path):
+    d = G.load(case)
+    M = G.n_instances(d)
+    e = _engine([_spec(d)] * M, path, glow=True, resort_interval=3)
+    _load_golden(e, d)
+    e.time = d["t0"]
+    done = 0
+    for cp in d["checkpoints"]:
+        e.step(int(cp) - done)
+        done = int(cp)
+        assert e.time == d[f"time_{cp}"]
+        for m in range(M):
+            got = e.read(m)
+            live = d[f"in{m}_material"] >= 0
+            tag = f"{case}/{path}/inst{m}/step{cp}"
+            assert_positions_close(got["x"][live], d[f"s{cp}_{m}_x"][live], 4 * int(cp), tag + " x")
+            for k in ("v", "C", "F", "Jp", "glow"):
+                assert_norm_close(got[k][live], d[f"s{cp}_{m}_{k}"][live], FIELD_RTOL, f"{tag} {k}")
+            assert np.array_equal(got["x"][~live], d[f"s{cp}_{m}_x"][~live])
+            assert_norm_close(got["glow"], d[f"s{cp}_{m}_glow"], FIELD_RTOL, f"{tag} glow(all)")
+            gv, gm = e.read_grid(m)
+            rv, rm = G.dense_grid(d, cp, m)
+            assert_norm_close(gm, rm, FIELD_RTOL, f"{tag} grid_m")
+            assert_norm_close(gv, rv, FIELD_RTOL, f"{tag} grid_v")
+            assert np.array_equal(gm > 0, rm > 0), f"{tag} grid occupancy"
+    assert not e.error_flags().any()
+    e.close()
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_headless_and_stats_match_reference(path):
+    d = G.load("headless_3inst")
+    M = G.n_instances(d)
+    e = _engine([_spec(d)] * M, path)
+    for m in range(M):
+        e.load(m, d[f"in{m}_x"], d[f"in{m}_material"], d[f"in{m}_fiber"])
+    e.set_params(**{k: d[f"param_{k}"] for k in ("actuation", "contraction", "freq", "payload_density")})
+    rtol = 2000 * 2.0 ** -24  # the reference sums in FP32 (see test_oracle_golden)
+    np.testing.assert_allclose(e.payload_stats(), d["payload_stats_before"], rtol=rtol)
+    np.testing.assert_allclose(e.stats_any(), d["stats_any_before"], rtol=rtol)
+    res = e.run_headless(int(d["checkpoints"][-1]))
+    np.testing.assert_allclose(res, d["headless"], rtol=rtol)
+    assert list(res[:, 4]) == [1.0, 1.0, 0.0]
+    assert e.time == d["time_after"]
+    np.testing.assert_allclose(e.payload_stats(), d["payload_stats_after"], rtol=rtol)
+    raw = e.stats_raw()
+    assert raw[1, 1] == 0 and raw[1, 4] > 0  # no payload in instance 1: body sums only
+    e.close()
+
+
+def _tank_instance(seed, n_slots=80000, grid=128, ny=128, dh=1.0, spawn=None, jitter=0.25):
+    from jellyfih_b200 import tank
+    g = tank.uniform_genomes(1, seed)[0]
+    pos, mat, fib, st = tank.fill_tank(g, n_slots, grid_res=grid, domain_height=dh,
+                                       spawn_offset=spawn, jitter=jitter, seed=seed)
+    c, f = tank.timing_params(g)
+    return pos, mat, fib, st, c, f
+
+
+def _oracle_run(pos, mat, fib, c, f, steps, nx=128, ny=128, dh=1.0, act=500.0, pdens=2.5):
+    from oracle import oracle as O
+    s = O.new_state(pos, mat, fib, "f32", nx, ny)
+    inst = O.Instance(nx=nx, ny=ny, domain_h=dh, contraction=c, freq=f, actuation=act,
+                      payload_density=pdens)
+    x0 = O.stats_any([s["x"]], [s["material"]])
+    O.run(inst, s, np.float32(0), steps)
+    x1 = O.stats_any([s["x"]], [s["material"]])
+    return s, O.headless_rows(x0, x1)[0]
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_full_tank_1000_steps_against_oracle(path):
+    """Config-1 workload: 1 instance, 80K slots, 128^2, 1,000 substeps."""
+    pos, mat, fib, st, c, f = _tank_instance(11)
+    from jellyfih_b200 import InstanceSpec
+    e = _engine([InstanceSpec(80000)], path)
+    e.load(0, pos, mat, fib)
+    e.set_params(contraction=[c], freq=[f])
+    res = e.run_headless(1000)[0]
+    s, ref = _oracle_run(pos, mat, fib, c, f, 1000)
+    disp, ref_disp = res[2] - res[0], ref[2] - ref[0]
+    assert res[4] == ref[4] == 1.0
+    assert abs(res[0] - ref[0]) <= 1e-7 * abs(ref[0])
+    # summation-order band of the FP32 system itself is ~0.7% at 1,000 steps
+    assert abs(disp - ref_disp) <= 0.03 * abs(ref_disp), (disp, ref_disp)
+    got = e.read(0)
+    live = mat >= 0
+    assert np.abs(got["x"][live] - s["x"][live]).max() < 2e-4
+    assert not e.error_flags().any()
+    e.close()
+
+
+def test_batched_uneven_instances_against_oracle():
+    """Mixed 128^2 / 128x256 / 64^2 instances in one batched launch, 200 substeps."""
+    from jellyfih_b200 import InstanceSpec, tank
+    cases = [dict(seed=21), dict(seed=22, n_slots=60000),
+             dict(seed=23, n_slots=160000, ny=256, dh=2.0, spawn=tank.TALL_SPAWN),
+             dict(seed=24, n_slots=24000, grid=64, ny=64)]
+    specs, data = [], []
+    for cfg in cases:
+        pos, mat, fib, st, c, f = _tank_instance(**cfg)
+        specs.append(InstanceSpec(cfg.get("n_slots", 80000), cfg.get("grid", 128), cfg.get("ny", 128),
+                                  cfg.get("dh", 1.0)))
+        data.append((pos, mat, fib, c, f))
+    e = _engine(specs, "batched", resort_interval=8)
+    acts = np.array([500.0, 900.0, 700.0, 300.0], np.float32)
+    for m, (pos, mat, fib, c, f) in enumerate(data):
+        e.load(m, pos, mat, fib)
+    e.set_params(actuation=acts, contraction=[d[3] for d in data], freq=[d[4] for d in data])
+    e.time = 0.0
+    e.step(200)
+    for m, (pos, mat, fib, c, f) in enumerate(data):
+        sp = specs[m]
+        s, _ = _oracle_run(pos, mat, fib, c, f, 200, sp.n_grid, sp.n_grid_y, sp.domain_height, acts[m])
+        got = e.read(m)
+        live = mat >= 0
+        assert np.abs(got["x"][live] - s["x"][live]).max() < 2e-5, m
+        assert_norm_close(got["v"][live], s["v"][live], 2e-2, f"inst{m} v")
+        assert_norm_close(got["F"][live], s["F"][live], 1e-4, f"inst{m} F")
+    e.close()
+
+
+def test_resort_interval_and_drift_beyond_halo():
+    """Fast particles cross several grid rows between re-sorts: the batched
+    path must route their scatter and gather through their rows' owners and
+    agree with the plain path."""
+    from jellyfih_b200 import InstanceSpec
+    pos, mat, fib, st, c, f = _tank_instance(31, n_slots=80000)
+    rng = np.random.default_rng(0)
+    v = np.zeros((80000, 2), np.float32)
+    live = mat >= 0
+    v[live] = rng.normal(0, 40.0, (live.sum(), 2)).astype(np.float32)  # ~1 cell per 10 substeps
+    outs = {}
+    for path, ri in (("plain", 16), ("batched", 1), ("batched", 64)):
+        e = _engine([InstanceSpec(80000)], path, resort_interval=ri)
+        e.load(0, pos, mat, fib)
+        e.write(0, v=v)
+        e.set_params(contraction=[c], freq=[f])
+        e.step(64)
+        outs[(path, ri)] = e.read(0)
+        assert not e.error_flags().any()
+        e.close()
+    ref = outs[("plain", 16)]
+    for key in (("batched", 1), ("batched", 64)):
+        got = outs[key]
+        assert np.abs(got["x"][live] - ref["x"][live]).max() < 1e-5, key
+        assert_norm_close(got["v"][live], ref["v"][live], 1e-3, f"{key} v")
+
+
+def test_nonfinite_flag_and_invalid_arguments():
+    from jellyfih_b200 import InstanceSpec, JfError
+    e = _engine([InstanceSpec(1000), InstanceSpec(1000)], "batched")
+    pos = np.full((1000, 2), 0.5, np.float32)
+    pos[:, 0] = np.linspace(0.3, 0.7, 1000)
+    mat = np.zeros(1000, np.int32)
+    e.load(0, pos, mat)
+    e.load(1, pos, mat)
+    v = np.zeros((1000, 2), np.float32)
+    v[10] = np.nan
+    e.write(1, v=v)
+    e.step(2)
+    flags = e.error_flags()
+    assert flags[0] == 0 and flags[1] != 0
+    e.clear_error_flags()
+    assert not e.error_flags().any()
+    with pytest.raises(JfError):
+        e.load(5, pos, mat)
+    with pytest.raises(JfError):
+        e.load(0, np.zeros((2000, 2), np.float32), np.zeros(2000, np.int32))
+    with pytest.raises(JfError):
+        e.step(-1)
+    e.close()
+
+
+def test_mpm_sim_module_drop_in(monkeypatch):
+    """The drop-in module runs the reference's evolve.py-style call sequence."""
+    import importlib
+    import sys
+    monkeypatch.setenv("JELLY_INSTANCES", "2")
+    monkeypatch.setenv("JELLY_PARTICLES", "80000")
+    sys.modules.pop("jellyfih_b200.mpm_sim", None)
+    sim = importlib.import_module("jellyfih_b200.mpm_sim")
+    from jellyfih_b200 import tank
+    for i, g in enumerate(tank.uniform_genomes(2, 41)):
+        pos, mat, fib, st = tank.fill_tank(g, sim.n_particles, grid_res=int(sim.n_grid))
+        sim.load_particles(i, pos, mat, fib)
+        sim.instance_act_contraction[i] = float(np.clip(g[9], 0.05, 0.60))
+        sim.instance_freq[i] = float(np.clip(g[10], 0.5, 2.0))
+    sim.ti.sync()
+    assert sim.instance_actuation[0] == 500.0 and sim.instance_payload_density[1] == 2.5
+    res = sim.run_batch_headless(50)
+    assert res.shape == (2, 5) and np.all(res[:, 4] == 1.0)
+    assert sim.sim_time[None] == pytest.approx(50 * 2e-5, rel=1e-6)
+    sim.clear_fitness_buffer()
+    sim.compute_payload_stats()
+    fb = sim.fitness_buffer.to_numpy()
+    np.testing.assert_allclose(fb[:, 0] / fb[:, 1], res[:, 2], rtol=1e-12)
+    assert sim.x.to_numpy().shape == (2, 80000, 2)
+    assert sim.grid_m.to_numpy().shape == (2, 128, 128)
+    sim.substep()
+    sim.engine().close()
+    sys.modules.pop("jellyfih_b200.mpm_sim", None)

@@ -39,16 +39,66 @@ struct ChunkArgs {
   float* Jp;
   const float2* fiber;
   float* glow;
-  const int32_t* band;   // M x (CS + 1) engine positions
-  float4* grid;          // grid of the chunk's last substep, node = g_off + j * nx + i
+  const int32_t* cell_end;  // M x stride: end of each cell's run (relative to p_off)
+  int32_t stride;
+  float4* grid;             // grid of the chunk's last substep, node = g_off + j * nx + i
   int32_t* err;
   int32_t M;
   int32_t CS;
-  int32_t K;             // substeps in this chunk
+  int32_t K;                // substeps in this chunk
   float t0;
   float dt;
   int32_t do_glow;
 };
+
+// Shared-memory window of one CTA: grid rows [win0, win0 + WR) of its
+// instance, planar (updated velocity Gx, Gy; accumulated momentum Ax, Ay and
+// mass Am).  Rows outside the window are reached in the owner CTA's window.
+struct Window {
+  float *Gx, *Gy, *Ax, *Ay, *Am;
+  int nx, H, win0, WR;
+};
+
+__device__ __forceinline__ int owner_of(const Window& w, int j) { return j / w.H; }
+__device__ __forceinline__ int owner_row(const Window& w, int j, int o) { return j - (o * w.H - kHaloLo); }
+
+__device__ __forceinline__ float2 gather_node(const Window& w, cg::cluster_group& cl, int i, int j) {
+  const int wr = j - w.win0;
+  if (wr >= 0 && wr < w.WR) {
+    const int n = wr * w.nx + i;
+    return make_float2(w.Gx[n], w.Gy[n]);
+  }
+  const int o = owner_of(w, j);
+  const int n = owner_row(w, j, o) * w.nx + i;
+  return make_float2(cl.map_shared_rank(w.Gx, o)[n], cl.map_shared_rank(w.Gy, o)[n]);
+}
+
+// Scatter of one particle's 9 stencil contributions with atomics, local when
+// the rows are in this CTA's window, else into the owner CTA's window.
+__device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_group& cl, const JfInst& I,
+                                                 const JfStencil& st, const JfScatter& sc) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int row = st.by + j;
+    const int wr = row - w.win0;
+    float *px = w.Ax, *py = w.Ay, *pm = w.Am;
+    int rn = wr * w.nx;
+    if (!(wr >= 0 && wr < w.WR)) {
+      const int o = owner_of(w, row);
+      px = cl.map_shared_rank(w.Ax, o);
+      py = cl.map_shared_rank(w.Ay, o);
+      pm = cl.map_shared_rank(w.Am, o);
+      rn = owner_row(w, row, o) * w.nx;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float3 c = jf_node_contrib(I, st, sc, i, j);
+      atomicAdd(px + rn + st.bx + i, c.x);
+      atomicAdd(py + rn + st.bx + i, c.y);
+      atomicAdd(pm + rn + st.bx + i, c.z);
+    }
+  }
+}
 
 __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   extern __shared__ float4 smem4[];
@@ -63,41 +113,67 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
 
   const JfInst I = a.inst[m];
   const JfParams P = a.params[m];
-  const JfMaterials mats = a.mats;  // a register copy: no address taken in parameter space
+  const JfMaterials mats = a.mats;
   const int nx = I.nx, ny = I.ny, H = I.band_h;
   const int row0 = r * H;
   const int own_hi = min(row0 + H, ny);
-  const int win0 = row0 - kHaloLo;
-  const int WR = H + kHalo;
-  const int WN = WR * nx;
-  float* Gx = sm;
-  float* Gy = Gx + WN;
-  float* Ax = Gy + WN;
-  float* Ay = Ax + WN;
-  float* Am = Ay + WN;
+  Window w;
+  w.nx = nx;
+  w.H = H;
+  w.win0 = row0 - kHaloLo;
+  w.WR = H + kHalo;
+  const int WN = w.WR * nx;
+  w.Gx = sm;
+  w.Gy = w.Gx + WN;
+  w.Ax = w.Gy + WN;
+  w.Ay = w.Ax + WN;
+  w.Am = w.Ay + WN;
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int lo = a.band[m * (CS + 1) + r];
-  const int hi = a.band[m * (CS + 1) + r + 1];
+  const int lane = tid & 31, warp = tid >> 5, n_warps = nth >> 5;
+  const int cells = nx * ny;
+  const int32_t* cend = a.cell_end + (int64_t)m * a.stride;
+  const int64_t p0 = I.p_off;
 
   for (int n = tid; n < 5 * WN; n += nth) sm[n] = 0.0f;
   cluster.sync();
 
-  // window position of grid row j in the CTA that owns it
-  auto owner_of = [&](int j) { return j / H; };
-  auto owner_row = [&](int j, int o) { return j - (o * H - kHaloLo); };
-
-  auto gather = [&](int ni, int nj) -> float2 {
-    const int wr = nj - win0;
-    if (wr >= 0 && wr < WR) {
-      const int n = wr * nx + ni;
-      return make_float2(Gx[n], Gy[n]);
+  // G2P of the previous substep, then P2G of this one, for a particle that
+  // is not handled by a cell lane (generic gathers and scatters).
+  auto particle_generic = [&](int64_t g, bool do_g2p, bool do_p2g, float pressure) {
+    const float4 xv = a.xv[g];
+    float4 C = a.C[g];
+    const int mt = a.mat[g];
+    float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+    float jp = 1.0f;
+    if (mt == 2 || a.do_glow) jp = a.Jp[g];
+    if (do_g2p) {
+      jf_g2p_particle(I, x, v, C, [&](int ni, int nj) { return gather_node(w, cluster, ni, nj); });
+      if (a.do_glow) a.glow[g] = jf_glow(a.glow[g], jp);
+      if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
+      a.xv[g] = make_float4(x.x, x.y, v.x, v.y);
+      a.C[g] = C;
     }
-    const int o = owner_of(nj);
-    const int n = owner_row(nj, o) * nx + ni;
-    const float* rx = cluster.map_shared_rank(Gx, o);
-    const float* ry = cluster.map_shared_rank(Gy, o);
-    return make_float2(rx[n], ry[n]);
+    if (do_p2g) {
+      JfStencil st;
+      if (jf_stencil(I, x, st)) {
+        float4 F = a.F[g];
+        const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+        JfScatter sc;
+        jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
+        a.F[g] = F;
+        if (mt == 2) a.Jp[g] = jp;
+        scatter_particle(w, cluster, I, st, sc);
+      }
+    }
   };
+
+  const int segs = (nx + 31) >> 5;
+  const int n_tasks = max(own_hi - row0, 0) * segs;
+  int oor_beg = 0, oor_end = 0;
+  if (r == CS - 1) {
+    oor_beg = cend[cells - 1];
+    oor_end = cend[cells];
+  }
 
   float t = a.t0;
   for (int s = 0; s <= a.K; ++s) {
@@ -107,92 +183,131 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     __syncthreads();
     const float pressure = s_pressure;
 
-    for (int k = lo + tid; k < hi; k += nth) {
-      const float4 xv = a.xv[k];
-      float4 C = a.C[k];
-      const int mt = a.mat[k];
-      float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
-      float jp = 1.0f;
-      if (mt == 2 || a.do_glow) jp = a.Jp[k];
-      if (do_g2p) {
-        jf_g2p_particle(I, x, v, C, gather);
-        if (a.do_glow) a.glow[k] = jf_glow(a.glow[k], jp);
-        if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
+    // cells of the band: a warp takes 32 consecutive cells of one row
+    for (int task = warp; task < n_tasks; task += n_warps) {
+      const int cy = row0 + task / segs;
+      const int seg0 = (task % segs) << 5;
+      const int cx = seg0 + lane;
+      int beg = 0, end = 0;
+      if (cx < nx) {
+        const int c = cy * nx + cx;
+        end = cend[c];
+        beg = c > 0 ? cend[c - 1] : 0;
       }
-      if (do_p2g) {
-        JfStencil st;
-        if (jf_stencil(I, x, st)) {
-          float4 F = a.F[k];
-          const float2 fb = (mt == 3) ? a.fiber[k] : make_float2(0.0f, 1.0f);
-          JfScatter sc;
-          jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
-          a.F[k] = F;
-          if (mt == 2) a.Jp[k] = jp;
-          const int wr0 = st.by - win0;
-          if (wr0 >= 0 && wr0 + 2 < WR) {
-            const int base = wr0 * nx + st.bx;
+      float acc[27];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
+      for (int q = 0; q < 27; ++q) acc[q] = 0.0f;
+      float2 gn[9];
+      if (do_g2p && end > beg && cx <= nx - 3 && cy <= ny - 3) {
 #pragma unroll
-              for (int i = 0; i < 3; ++i) {
-                const float3 c = jf_node_contrib(I, st, sc, i, j);
-                const int n = base + j * nx + i;
-                atomicAdd(Ax + n, c.x);
-                atomicAdd(Ay + n, c.y);
-                atomicAdd(Am + n, c.z);
-              }
+        for (int j = 0; j < 3; ++j) {
+          const int rowo = (cy + j - w.win0) * nx + cx;
+#pragma unroll
+          for (int i = 0; i < 3; ++i) gn[j * 3 + i] = make_float2(w.Gx[rowo + i], w.Gy[rowo + i]);
+        }
+      }
+      for (int k = beg; k < end; ++k) {
+        const int64_t g = p0 + k;
+        const float4 xv = a.xv[g];
+        float4 C = a.C[g];
+        const int mt = a.mat[g];
+        float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+        float jp = 1.0f;
+        if (mt == 2 || a.do_glow) jp = a.Jp[g];
+        if (do_g2p) {
+          JfStencil st;
+          if (jf_stencil(I, x, st)) {
+            if (st.bx == cx && st.by == cy) {
+              jf_g2p_apic(I, st, v, C, [&](int i, int j) { return gn[j * 3 + i]; });
+            } else {
+              jf_g2p_apic(I, st, v, C,
+                          [&](int i, int j) { return gather_node(w, cluster, st.bx + i, st.by + j); });
             }
-          } else {
+          }
+          jf_g2p_advect(I, x, v);
+          if (a.do_glow) a.glow[g] = jf_glow(a.glow[g], jp);
+          if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
+          a.xv[g] = make_float4(x.x, x.y, v.x, v.y);
+          a.C[g] = C;
+        }
+        if (do_p2g) {
+          JfStencil st;
+          if (jf_stencil(I, x, st)) {
+            float4 F = a.F[g];
+            const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+            JfScatter sc;
+            jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
+            a.F[g] = F;
+            if (mt == 2) a.Jp[g] = jp;
+            if (st.bx == cx && st.by == cy) {
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-              const int row = st.by + j;
-              const int wr = row - win0;
-              float *px, *py, *pm;
-              int rn;
-              if (wr >= 0 && wr < WR) {
-                px = Ax; py = Ay; pm = Am;
-                rn = wr * nx;
-              } else {
-                const int o = owner_of(row);
-                px = cluster.map_shared_rank(Ax, o);
-                py = cluster.map_shared_rank(Ay, o);
-                pm = cluster.map_shared_rank(Am, o);
-                rn = owner_row(row, o) * nx;
-              }
+              for (int j = 0; j < 3; ++j) {
 #pragma unroll
-              for (int i = 0; i < 3; ++i) {
-                const float3 c = jf_node_contrib(I, st, sc, i, j);
-                atomicAdd(px + rn + st.bx + i, c.x);
-                atomicAdd(py + rn + st.bx + i, c.y);
-                atomicAdd(pm + rn + st.bx + i, c.z);
+                for (int i = 0; i < 3; ++i) {
+                  const float3 c = jf_node_contrib(I, st, sc, i, j);
+                  acc[(j * 3 + i) * 3 + 0] += c.x;
+                  acc[(j * 3 + i) * 3 + 1] += c.y;
+                  acc[(j * 3 + i) * 3 + 2] += c.z;
+                }
               }
+            } else {
+              scatter_particle(w, cluster, I, st, sc);
             }
           }
         }
       }
-      if (do_g2p) {
-        a.xv[k] = make_float4(x.x, x.y, v.x, v.y);
-        a.C[k] = C;
+      __syncwarp();
+      if (do_p2g) {
+        // merge the overlapping columns of neighbouring cells along x, then one
+        // atomic per lane and (row, component); lanes 30 and 31 also own the
+        // two columns past the segment
+        const bool edge_ok = seg0 + 32 < nx;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const int rowo = (cy + j - w.win0) * nx;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            float* A = q == 0 ? w.Ax : (q == 1 ? w.Ay : w.Am);
+            const float a0 = acc[(j * 3 + 0) * 3 + q];
+            const float a1 = acc[(j * 3 + 1) * 3 + q];
+            const float a2 = acc[(j * 3 + 2) * 3 + q];
+            const float u1 = __shfl_up_sync(0xffffffffu, a1, 1);
+            const float u2 = __shfl_up_sync(0xffffffffu, a2, 2);
+            const float l30 = __shfl_sync(0xffffffffu, a2, 30);
+            float col = a0;
+            if (lane >= 1) col += u1;
+            if (lane >= 2) col += u2;
+            if (cx < nx && col != 0.0f) atomicAdd(A + rowo + cx, col);
+            if (lane == 31 && edge_ok) {
+              const float e32 = a1 + l30;
+              if (e32 != 0.0f) atomicAdd(A + rowo + seg0 + 32, e32);
+              if (seg0 + 33 < nx && a2 != 0.0f) atomicAdd(A + rowo + seg0 + 33, a2);
+            }
+          }
+        }
       }
     }
+    // live particles outside every stencil range (last band only)
+    for (int k = oor_beg + tid; k < oor_end; k += nth)
+      particle_generic(p0 + k, do_g2p, do_p2g, pressure);
     __syncthreads();
 
     if (do_p2g) {
       // halo rows of the accumulator go to the rows' owners
       for (int n = tid; n < WN; n += nth) {
         const int wr = n / nx;
-        const int j = win0 + wr;
+        const int j = w.win0 + wr;
         if ((j >= row0 && j < own_hi) || j < 0 || j >= ny) continue;
-        const float vx = Ax[n], vy = Ay[n], vm = Am[n];
+        const float vx = w.Ax[n], vy = w.Ay[n], vm = w.Am[n];
         if (vx != 0.0f || vy != 0.0f || vm != 0.0f) {
-          const int o = owner_of(j);
-          const int rn = owner_row(j, o) * nx + (n - wr * nx);
-          atomicAdd(cluster.map_shared_rank(Ax, o) + rn, vx);
-          atomicAdd(cluster.map_shared_rank(Ay, o) + rn, vy);
-          atomicAdd(cluster.map_shared_rank(Am, o) + rn, vm);
-          Ax[n] = 0.0f;
-          Ay[n] = 0.0f;
-          Am[n] = 0.0f;
+          const int o = owner_of(w, j);
+          const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
+          atomicAdd(cluster.map_shared_rank(w.Ax, o) + rn, vx);
+          atomicAdd(cluster.map_shared_rank(w.Ay, o) + rn, vy);
+          atomicAdd(cluster.map_shared_rank(w.Am, o) + rn, vm);
+          w.Ax[n] = 0.0f;
+          w.Ay[n] = 0.0f;
+          w.Am[n] = 0.0f;
         }
       }
       cluster.sync();
@@ -203,27 +318,27 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       for (int n = kHaloLo * nx + tid; n < n_end; n += nth) {
         const int wr = n / nx;
         const int i = n - wr * nx;
-        const int j = win0 + wr;
-        const float mm = Am[n];
-        const float2 u = jf_grid_node(I, i, j, Ax[n], Ay[n], mm);
-        Gx[n] = u.x;
-        Gy[n] = u.y;
+        const int j = w.win0 + wr;
+        const float mm = w.Am[n];
+        const float2 u = jf_grid_node(I, i, j, w.Ax[n], w.Ay[n], mm);
+        w.Gx[n] = u.x;
+        w.Gy[n] = u.y;
         if (last) a.grid[I.g_off + (int64_t)j * nx + i] = make_float4(u.x, u.y, mm, 0.0f);
-        Ax[n] = 0.0f;
-        Ay[n] = 0.0f;
-        Am[n] = 0.0f;
+        w.Ax[n] = 0.0f;
+        w.Ay[n] = 0.0f;
+        w.Am[n] = 0.0f;
       }
       cluster.sync();
 
       // halo rows of the updated grid come from their owners
       for (int n = tid; n < WN; n += nth) {
         const int wr = n / nx;
-        const int j = win0 + wr;
+        const int j = w.win0 + wr;
         if ((j >= row0 && j < own_hi) || j < 0 || j >= ny) continue;
-        const int o = owner_of(j);
-        const int rn = owner_row(j, o) * nx + (n - wr * nx);
-        Gx[n] = cluster.map_shared_rank(Gx, o)[rn];
-        Gy[n] = cluster.map_shared_rank(Gy, o)[rn];
+        const int o = owner_of(w, j);
+        const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
+        w.Gx[n] = cluster.map_shared_rank(w.Gx, o)[rn];
+        w.Gy[n] = cluster.map_shared_rank(w.Gy, o)[rn];
       }
       __syncthreads();
       t = t + a.dt;
@@ -390,7 +505,8 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.Jp = e->p.Jp;
   a.fiber = e->p.fiber;
   a.glow = e->p.glow;
-  a.band = e->d_band;
+  a.cell_end = e->d_counts;
+  a.stride = e->max_cells + 2;
   a.grid = e->d_grid;
   a.err = e->d_err;
   a.M = e->M;

@@ -258,35 +258,36 @@ __device__ __forceinline__ float2 jf_grid_node(const JfInst& I, int i, int j, fl
   return make_float2(g0, g1);
 }
 
-// G2P for one particle (mpm_sim.py:315-333): APIC gather of v and C from the
-// updated grid when the stencil is in range, then gravity, advection and the
-// wall clamp for every live particle.  `gather(i_node, j_node)` returns the
-// updated grid velocity of a node.
+// APIC gather of G2P (mpm_sim.py:317-327) for a particle whose stencil is in
+// range: new v and C from the updated grid.  `gather(i, j)` returns the
+// updated velocity of stencil node (bx + i, by + j), i, j in 0..2.
 template <class Gather>
-__device__ __forceinline__ void jf_g2p_particle(const JfInst& I, float2& x, float2& v, float4& C,
-                                                Gather gather) {
-  JfStencil st;
-  if (jf_stencil(I, x, st)) {
-    float nv0 = 0.f, nv1 = 0.f, c00 = 0.f, c01 = 0.f, c10 = 0.f, c11 = 0.f;
+__device__ __forceinline__ void jf_g2p_apic(const JfInst& I, const JfStencil& st, float2& v, float4& C,
+                                            Gather gather) {
+  float nv0 = 0.f, nv1 = 0.f, c00 = 0.f, c01 = 0.f, c10 = 0.f, c11 = 0.f;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
+  for (int i = 0; i < 3; ++i) {
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        float d0 = (float)i - st.fx0, d1 = (float)j - st.fx1;
-        float2 g = gather(st.bx + i, st.by + j);
-        float weight = jf_w(st, 0, i) * jf_w(st, 1, j);
-        nv0 = nv0 + weight * g.x;
-        nv1 = nv1 + weight * g.y;
-        float k = I.c4 * weight;
-        c00 = c00 + k * (g.x * d0);
-        c01 = c01 + k * (g.x * d1);
-        c10 = c10 + k * (g.y * d0);
-        c11 = c11 + k * (g.y * d1);
-      }
+    for (int j = 0; j < 3; ++j) {
+      float d0 = (float)i - st.fx0, d1 = (float)j - st.fx1;
+      float2 g = gather(i, j);
+      float weight = jf_w(st, 0, i) * jf_w(st, 1, j);
+      nv0 = nv0 + weight * g.x;
+      nv1 = nv1 + weight * g.y;
+      float k = I.c4 * weight;
+      c00 = c00 + k * (g.x * d0);
+      c01 = c01 + k * (g.x * d1);
+      c10 = c10 + k * (g.y * d0);
+      c11 = c11 + k * (g.y * d1);
     }
-    v = make_float2(nv0, nv1);
-    C = make_float4(c00, c01, c10, c11);
   }
+  v = make_float2(nv0, nv1);
+  C = make_float4(c00, c01, c10, c11);
+}
+
+// Gravity, advection and the wall clamp of every live particle
+// (mpm_sim.py:329-333).
+__device__ __forceinline__ void jf_g2p_advect(const JfInst& I, float2& x, float2& v) {
   v.y = v.y - I.dtg;
   // rounded as the reference rounds it (product, then sum): a fused
   // multiply-add here shifts 1,000-step payload displacement by ~0.2%
@@ -294,6 +295,18 @@ __device__ __forceinline__ void jf_g2p_particle(const JfInst& I, float2& x, floa
   x.y = __fadd_rn(x.y, __fmul_rn(I.dt, v.y));
   x.x = fmaxf(fminf(x.x, 0.999f), 0.001f);
   x.y = fmaxf(fminf(x.y, I.y_hi), 0.001f);
+}
+
+// G2P for one particle (mpm_sim.py:315-333).  `gather(i_node, j_node)`
+// returns the updated grid velocity of an absolute node.
+template <class Gather>
+__device__ __forceinline__ void jf_g2p_particle(const JfInst& I, float2& x, float2& v, float4& C,
+                                                Gather gather) {
+  JfStencil st;
+  if (jf_stencil(I, x, st)) {
+    jf_g2p_apic(I, st, v, C, [&](int i, int j) { return gather(st.bx + i, st.by + j); });
+  }
+  jf_g2p_advect(I, x, v);
 }
 
 // visual_glow decay (mpm_sim.py:336-338), render-only.

@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
   __shared__ float s_pressure;
+  __shared__ int s_next_task;
 
   cg::cluster_group cluster = cg::this_cluster();
   const int CS = a.CS;
@@ -133,6 +134,11 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const int cells = nx * ny;
   const int32_t* cend = a.cell_end + (int64_t)m * a.stride;
   const int64_t p0 = I.p_off;
+  // this instance's particle arrays, indexed by position within the instance
+  float4* __restrict__ xv_m = a.xv + p0;
+  float4* __restrict__ C_m = a.C + p0;
+  float4* __restrict__ F_m = a.F + p0;
+  const int32_t* __restrict__ mat_m = a.mat + p0;
 
   for (int n = tid; n < 5 * WN; n += nth) sm[n] = 0.0f;
   cluster.sync();
@@ -183,8 +189,11 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     __syncthreads();
     const float pressure = s_pressure;
 
-    // cells of the band: a warp takes 32 consecutive cells of one row
-    for (int task = warp; task < n_tasks; task += n_warps) {
+    // cells of the band: a warp takes 32 consecutive cells of one row; warps
+    // claim row segments from a shared counter so that they finish together
+    if (tid == 0) s_next_task = n_warps;
+    __syncthreads();
+    for (int task = warp; task < n_tasks;) {
       const int cy = row0 + task / segs;
       const int seg0 = (task % segs) << 5;
       const int cx = seg0 + lane;
@@ -197,48 +206,57 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       float acc[27];
 #pragma unroll
       for (int q = 0; q < 27; ++q) acc[q] = 0.0f;
-      float2 gn[9];
-      if (do_g2p && end > beg && cx <= nx - 3 && cy <= ny - 3) {
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int rowo = (cy + j - w.win0) * nx + cx;
-#pragma unroll
-          for (int i = 0; i < 3; ++i) gn[j * 3 + i] = make_float2(w.Gx[rowo + i], w.Gy[rowo + i]);
-        }
+      // window offset of the lane cell's stencil origin
+      const int wbase = (cy - w.win0) * nx + cx;
+      float4 nxv, nC, nF;
+      int nmt = -1;
+      if (beg < end) {
+        nxv = xv_m[beg];
+        nC = C_m[beg];
+        nmt = mat_m[beg];
+        nF = F_m[beg];
       }
       for (int k = beg; k < end; ++k) {
-        const int64_t g = p0 + k;
-        const float4 xv = a.xv[g];
-        float4 C = a.C[g];
-        const int mt = a.mat[g];
+        const float4 xv = nxv;
+        float4 C = nC;
+        float4 F = nF;
+        const int mt = nmt;
+        if (k + 1 < end) {  // next particle of this cell, loaded while this one computes
+          nxv = xv_m[k + 1];
+          nC = C_m[k + 1];
+          nmt = mat_m[k + 1];
+          nF = F_m[k + 1];
+        }
         float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
         float jp = 1.0f;
-        if (mt == 2 || a.do_glow) jp = a.Jp[g];
+        if (mt == 2 || a.do_glow) jp = a.Jp[p0 + k];
         if (do_g2p) {
           JfStencil st;
           if (jf_stencil(I, x, st)) {
             if (st.bx == cx && st.by == cy) {
-              jf_g2p_apic(I, st, v, C, [&](int i, int j) { return gn[j * 3 + i]; });
+              jf_g2p_apic(I, st, v, C, [&](int i, int j) {
+                const int n = wbase + j * nx + i;
+                return make_float2(w.Gx[n], w.Gy[n]);
+              });
             } else {
               jf_g2p_apic(I, st, v, C,
                           [&](int i, int j) { return gather_node(w, cluster, st.bx + i, st.by + j); });
             }
           }
           jf_g2p_advect(I, x, v);
-          if (a.do_glow) a.glow[g] = jf_glow(a.glow[g], jp);
+          if (a.do_glow) a.glow[p0 + k] = jf_glow(a.glow[p0 + k], jp);
           if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
-          a.xv[g] = make_float4(x.x, x.y, v.x, v.y);
-          a.C[g] = C;
+          xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
+          C_m[k] = C;
         }
         if (do_p2g) {
           JfStencil st;
           if (jf_stencil(I, x, st)) {
-            float4 F = a.F[g];
-            const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+            const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
             JfScatter sc;
             jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
-            a.F[g] = F;
-            if (mt == 2) a.Jp[g] = jp;
+            F_m[k] = F;
+            if (mt == 2) a.Jp[p0 + k] = jp;
             if (st.bx == cx && st.by == cy) {
 #pragma unroll
               for (int j = 0; j < 3; ++j) {
@@ -259,8 +277,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       __syncwarp();
       if (do_p2g) {
         // merge the overlapping columns of neighbouring cells along x, then one
-        // atomic per lane and (row, component); lanes 30 and 31 also own the
-        // two columns past the segment
+        // atomic per lane and (row, component); lane 31 also owns the two
+        // columns past the segment
         const bool edge_ok = seg0 + 32 < nx;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
@@ -286,6 +304,9 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           }
         }
       }
+      int nt = 0;
+      if (lane == 0) nt = atomicAdd(&s_next_task, 1);
+      task = __shfl_sync(0xffffffffu, nt, 0);
     }
     // live particles outside every stencil range (last band only)
     for (int k = oor_beg + tid; k < oor_end; k += nth)

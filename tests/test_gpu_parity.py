@@ -267,7 +267,7 @@ def test_mpm_sim_module_drop_in(monkeypatch):
     sim.clear_fitness_buffer()
     sim.compute_payload_stats()
     fb = sim.fitness_buffer.to_numpy()
-    np.testing.assert_allclose(fb[:, 0] / fb[:, 1], res[:, 2], rtol=1e-12)
+    np.testing.assert_allclose(fb[:, 0] / fb[:, 1], res[:, 2], rtol=1e-6)  # FP32 field, as in the reference
     assert sim.x.to_numpy().shape == (2, 80000, 2)
     assert sim.grid_m.to_numpy().shape == (2, 128, 128)
     sim.substep()

@@ -28,6 +28,18 @@ constexpr int kHalo = kHaloLo + kHaloHi;
 constexpr int kSortThreads = 256;
 constexpr int kScanThreads = 1024;
 
+// Sort cell of a particle: (floor(X - 1/4), floor(Y - 1/4)) in grid units,
+// clamped at 0.  The stencil base trunc(X - 1/2) of a particle in sort cell k
+// is k - 1 or k, so a lane that owns cell k accumulates a 4x4 node block.
+// The reference's water lattice (spacing dx/2) puts half its lines exactly on
+// X - 1/2 in Z, where the base flips with any motion; the quarter shift keeps
+// every lattice point a quarter cell away from a sort-cell edge.
+__device__ __forceinline__ int2 sort_cell(const JfInst& I, float2 x) {
+  const int kx = max((int)floorf(x.x * I.inv_dx - 0.25f), 0);
+  const int ky = max((int)floorf(x.y * I.inv_dx - 0.25f), 0);
+  return make_int2(kx, ky);
+}
+
 struct ChunkArgs {
   const JfInst* inst;
   const JfParams* params;
@@ -96,6 +108,61 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
       atomicAdd(px + rn + st.bx + i, c.x);
       atomicAdd(py + rn + st.bx + i, c.y);
       atomicAdd(pm + rn + st.bx + i, c.z);
+    }
+  }
+}
+
+// Adds a particle's 3x3 stencil into the lane's 4x4 node block, shifted by
+// (DI, DJ) = stencil base - (cell - 1).
+template <int DI, int DJ>
+__device__ __forceinline__ void accumulate_block(float* acc, const JfInst& I, const JfStencil& st,
+                                                 const JfScatter& sc) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float3 c = jf_node_contrib(I, st, sc, i, j);
+      const int q = ((j + DJ) * 4 + (i + DI)) * 3;
+      acc[q + 0] += c.x;
+      acc[q + 1] += c.y;
+      acc[q + 2] += c.z;
+    }
+  }
+}
+
+// Writes a warp's 4x4 node blocks into the window.  Lane l owns cell column
+// cx = seg0 + l and covers node columns cx-1 .. cx+2; node column cx collects
+// block column 1 of lane l, 0 of lane l+1, 2 of lane l-1 and 3 of lane l-2,
+// so each lane issues one atomic per (row, component).  Lane 0 also writes
+// column seg0-1, lane 31 columns seg0+32 and seg0+33.
+__device__ __forceinline__ void flush_block(const float* acc, const Window& w, int lane, int cx, int cy,
+                                            int seg0, int nx) {
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int J = 0; J < 4; ++J) {
+    const int rowo = (cy - 1 + J - w.win0) * nx;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float* A = q == 0 ? w.Ax : (q == 1 ? w.Ay : w.Am);
+      const float a0 = acc[(J * 4 + 0) * 3 + q];
+      const float a1 = acc[(J * 4 + 1) * 3 + q];
+      const float a2 = acc[(J * 4 + 2) * 3 + q];
+      const float a3 = acc[(J * 4 + 3) * 3 + q];
+      const float from_right = __shfl_down_sync(full, a0, 1);
+      const float from_left = __shfl_up_sync(full, a2, 1);
+      const float from_left2 = __shfl_up_sync(full, a3, 2);
+      const float a3_l30 = __shfl_sync(full, a3, 30);
+      float col = a1;
+      if (lane <= 30) col += from_right;
+      if (lane >= 1) col += from_left;
+      if (lane >= 2) col += from_left2;
+      if (cx < nx && col != 0.0f) atomicAdd(A + rowo + cx, col);
+      if (lane == 0 && seg0 >= 1 && a0 != 0.0f) atomicAdd(A + rowo + seg0 - 1, a0);
+      if (lane == 31) {
+        const float e32 = a2 + a3_l30;
+        if (seg0 + 32 < nx && e32 != 0.0f) atomicAdd(A + rowo + seg0 + 32, e32);
+        if (seg0 + 33 < nx && a3 != 0.0f) atomicAdd(A + rowo + seg0 + 33, a3);
+      }
     }
   }
 }
@@ -203,11 +270,10 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         end = cend[c];
         beg = c > 0 ? cend[c - 1] : 0;
       }
-      float acc[27];
+      // 4x4 node block: columns cx-1 .. cx+2, rows cy-1 .. cy+2
+      float acc[48];
 #pragma unroll
-      for (int q = 0; q < 27; ++q) acc[q] = 0.0f;
-      // window offset of the lane cell's stencil origin
-      const int wbase = (cy - w.win0) * nx + cx;
+      for (int q = 0; q < 48; ++q) acc[q] = 0.0f;
       float4 nxv, nC, nF;
       int nmt = -1;
       if (beg < end) {
@@ -233,9 +299,11 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         if (do_g2p) {
           JfStencil st;
           if (jf_stencil(I, x, st)) {
-            if (st.bx == cx && st.by == cy) {
+            const int wr0 = st.by - w.win0;
+            if (wr0 >= 0 && wr0 + 2 < w.WR) {
+              const int wb = wr0 * nx + st.bx;
               jf_g2p_apic(I, st, v, C, [&](int i, int j) {
-                const int n = wbase + j * nx + i;
+                const int n = wb + j * nx + i;
                 return make_float2(w.Gx[n], w.Gy[n]);
               });
             } else {
@@ -257,17 +325,15 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
             jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
             F_m[k] = F;
             if (mt == 2) a.Jp[p0 + k] = jp;
-            if (st.bx == cx && st.by == cy) {
-#pragma unroll
-              for (int j = 0; j < 3; ++j) {
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                  const float3 c = jf_node_contrib(I, st, sc, i, j);
-                  acc[(j * 3 + i) * 3 + 0] += c.x;
-                  acc[(j * 3 + i) * 3 + 1] += c.y;
-                  acc[(j * 3 + i) * 3 + 2] += c.z;
-                }
-              }
+            const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
+            if (di == 0 && dj == 0) {
+              accumulate_block<0, 0>(acc, I, st, sc);
+            } else if (di == 1 && dj == 0) {
+              accumulate_block<1, 0>(acc, I, st, sc);
+            } else if (di == 0 && dj == 1) {
+              accumulate_block<0, 1>(acc, I, st, sc);
+            } else if (di == 1 && dj == 1) {
+              accumulate_block<1, 1>(acc, I, st, sc);
             } else {
               scatter_particle(w, cluster, I, st, sc);
             }
@@ -275,35 +341,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         }
       }
       __syncwarp();
-      if (do_p2g) {
-        // merge the overlapping columns of neighbouring cells along x, then one
-        // atomic per lane and (row, component); lane 31 also owns the two
-        // columns past the segment
-        const bool edge_ok = seg0 + 32 < nx;
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int rowo = (cy + j - w.win0) * nx;
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            float* A = q == 0 ? w.Ax : (q == 1 ? w.Ay : w.Am);
-            const float a0 = acc[(j * 3 + 0) * 3 + q];
-            const float a1 = acc[(j * 3 + 1) * 3 + q];
-            const float a2 = acc[(j * 3 + 2) * 3 + q];
-            const float u1 = __shfl_up_sync(0xffffffffu, a1, 1);
-            const float u2 = __shfl_up_sync(0xffffffffu, a2, 2);
-            const float l30 = __shfl_sync(0xffffffffu, a2, 30);
-            float col = a0;
-            if (lane >= 1) col += u1;
-            if (lane >= 2) col += u2;
-            if (cx < nx && col != 0.0f) atomicAdd(A + rowo + cx, col);
-            if (lane == 31 && edge_ok) {
-              const float e32 = a1 + l30;
-              if (e32 != 0.0f) atomicAdd(A + rowo + seg0 + 32, e32);
-              if (seg0 + 33 < nx && a2 != 0.0f) atomicAdd(A + rowo + seg0 + 33, a2);
-            }
-          }
-        }
-      }
+      if (do_p2g) flush_block(acc, w, lane, cx, cy, seg0, nx);
       int nt = 0;
       if (lane == 0) nt = atomicAdd(&s_next_task, 1);
       task = __shfl_sync(0xffffffffu, nt, 0);
@@ -386,7 +424,12 @@ __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* 
   } else {
     const float4 a = xv[g];
     JfStencil st;
-    key = jf_stencil(I, make_float2(a.x, a.y), st) ? st.by * I.nx + st.bx : cells;
+    if (jf_stencil(I, make_float2(a.x, a.y), st)) {
+      const int2 c = sort_cell(I, make_float2(a.x, a.y));
+      key = c.y * I.nx + c.x;
+    } else {
+      key = cells;
+    }
   }
   keys[g] = key;
   atomicAdd(counts + (int64_t)m * stride + key, 1);

@@ -256,6 +256,7 @@ def run_ours(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     engine.set_kernel_timing(True)
+    engine.path_counts(reset=True)
     launches0 = engine.kernel_launches
     with ClockSampler(local) as clocks:
         ev0.record(stream)
@@ -269,6 +270,7 @@ def run_ours(args):
     kt = engine.kernel_timing()
     engine.set_kernel_timing(False)
     gpu_launches = engine.kernel_launches - launches0
+    paths = engine.path_counts()
     flags = engine.error_flags()
     ms_max = allreduce(ms, dist.ReduceOp.MAX if world > 1 else None)
     live_total = allreduce(float(live), dist.ReduceOp.SUM if world > 1 else None)
@@ -287,6 +289,7 @@ def run_ours(args):
                 "kernel": "chunk_kernel", "algorithmic_bytes_per_launch": bytes_per_launch,
                 "mean_launch_ms": mean_launch_s * 1e3, "launches": kt["step_launches"],
                 "step_kernel_share": kt["step_ms"] / ms if ms > 0 else None,
+                "scatter_paths": paths,
                 "sort_ms": kt["sort_ms"], "sort_launches": kt["sort_launches"]}
 
     extras = {}

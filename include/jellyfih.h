@@ -129,6 +129,12 @@ int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m);
 int jf_error_flags(jf_engine* e, int32_t* out);
 int jf_clear_error_flags(jf_engine* e);
 
+/* Batched path counters since the last reset: out[0] particle scatters
+ * accumulated in a lane's register block, out[1] scatters through per-particle
+ * atomics (drifted or out-of-range particles), out[2] G2P gathers outside the
+ * CTA's shared-memory window.  All zero on the plain path. */
+int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset);
+
 /* Number of kernels this engine has launched. */
 int64_t jf_kernel_launches(const jf_engine* e);
 

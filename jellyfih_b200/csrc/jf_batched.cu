@@ -61,6 +61,7 @@ struct ChunkArgs {
   float t0;
   float dt;
   int32_t do_glow;
+  unsigned long long* path;  // [register scatters, generic scatters, generic gathers]
 };
 
 // Shared-memory window of one CTA: grid rows [win0, win0 + WR) of its
@@ -208,6 +209,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const int32_t* __restrict__ mat_m = a.mat + p0;
 
   for (int n = tid; n < 5 * WN; n += nth) sm[n] = 0.0f;
+  unsigned n_fast = 0, n_generic = 0, n_gather_generic = 0;
   cluster.sync();
 
   // G2P of the previous substep, then P2G of this one, for a particle that
@@ -307,6 +309,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
                 return make_float2(w.Gx[n], w.Gy[n]);
               });
             } else {
+              ++n_gather_generic;
               jf_g2p_apic(I, st, v, C,
                           [&](int i, int j) { return gather_node(w, cluster, st.bx + i, st.by + j); });
             }
@@ -326,6 +329,9 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
             F_m[k] = F;
             if (mt == 2) a.Jp[p0 + k] = jp;
             const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
+            const bool in_block = (unsigned)di < 2u && (unsigned)dj < 2u;
+            n_fast += in_block ? 1u : 0u;
+            n_generic += in_block ? 0u : 1u;
             if (di == 0 && dj == 0) {
               accumulate_block<0, 0>(acc, I, st, sc);
             } else if (di == 1 && dj == 0) {
@@ -347,8 +353,10 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       task = __shfl_sync(0xffffffffu, nt, 0);
     }
     // live particles outside every stencil range (last band only)
-    for (int k = oor_beg + tid; k < oor_end; k += nth)
+    for (int k = oor_beg + tid; k < oor_end; k += nth) {
       particle_generic(p0 + k, do_g2p, do_p2g, pressure);
+      ++n_generic;
+    }
     __syncthreads();
 
     if (do_p2g) {
@@ -401,6 +409,17 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       }
       __syncthreads();
       t = t + a.dt;
+    }
+  }
+  // path counters: one atomic per warp
+  if (a.path) {
+    const unsigned f = __reduce_add_sync(0xffffffffu, n_fast);
+    const unsigned g = __reduce_add_sync(0xffffffffu, n_generic);
+    const unsigned h = __reduce_add_sync(0xffffffffu, n_gather_generic);
+    if (lane == 0) {
+      atomicAdd(a.path + 0, (unsigned long long)f);
+      atomicAdd(a.path + 1, (unsigned long long)g);
+      atomicAdd(a.path + 2, (unsigned long long)h);
     }
   }
   // peers may still read this CTA's grid rows in their last G2P pass
@@ -579,6 +598,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.t0 = e->t;
   a.dt = (float)e->dt;
   a.do_glow = (e->flags & JF_FLAG_GLOW) ? 1 : 0;
+  a.path = e->d_path;
 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(e->M * e->cluster, 1, 1);

@@ -310,7 +310,9 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     if ((err = alloc_particles(e->q, p_off)) != cudaSuccess ||
         (err = alloc(&e->d_keys, p_off)) != cudaSuccess ||
         (err = alloc(&e->d_counts, (size_t)(e->max_cells + 2) * e->M)) != cudaSuccess ||
-        (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess)
+        (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_path, 4)) != cudaSuccess ||
+        (err = cudaMemset(e->d_path, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
       return bail(JF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
     if ((err = jf_batched_prepare(e)) != cudaSuccess)
       return bail(JF_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(err));
@@ -347,7 +349,7 @@ int jf_destroy(jf_engine* e) {
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_band); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
-  cudaFree(e->d_stage); cudaFree(e->d_stage_i);
+  cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   for (auto& pr : e->step_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto& pr : e->sort_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto ev : e->event_pool) cudaEventDestroy(ev);
@@ -586,6 +588,20 @@ int jf_clear_error_flags(jf_engine* e) {
 }
 
 int64_t jf_kernel_launches(const jf_engine* e) { return e ? e->launches : -1; }
+
+int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset) {
+  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  out[0] = out[1] = out[2] = 0;
+  if (!e->d_path) return JF_OK;
+  int rc = set_device(e);
+  if (rc) return rc;
+  unsigned long long h[4] = {0, 0, 0, 0};
+  JF_CK(cudaMemcpyAsync(h, e->d_path, sizeof(h), cudaMemcpyDeviceToHost, e->stream), "read path counters");
+  JF_CK(cudaStreamSynchronize(e->stream), "path counters sync");
+  for (int i = 0; i < 3; ++i) out[i] = (int64_t)h[i];
+  if (reset) JF_CK(cudaMemsetAsync(e->d_path, 0, sizeof(h), e->stream), "reset path counters");
+  return JF_OK;
+}
 
 int jf_set_kernel_timing(jf_engine* e, int32_t enable) {
   if (check_engine(e)) return JF_ERR_INVALID;

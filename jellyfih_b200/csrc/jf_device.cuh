@@ -1,9 +1,14 @@
 // Device math of the 2-D MLS-MPM substep, shared by the plain and batched
 // paths.  Each function follows the reference engine mpm_sim.py (line numbers
-// cited per function) in its operation order; FP32 throughout, with FMA
-// contraction left to the compiler except in the waveform phase, which is
-// rounded step by step so that the 1 -> 0 drop of the activation lands on the
-// same substep as in the reference.
+// cited per function) in its operation order, FP32 throughout.
+//
+// Rounding: the chain F update -> SVD -> plasticity -> stress -> APIC affine
+// ends in the cancellation F - R, so every operation there is rounded on its
+// own (the _rn intrinsics below), as the reference's FP32 arithmetic rounds
+// it; letting the compiler fuse multiply-adds in that chain moves a
+// substep's fields by ~1e-5.  The G2P gather, the node contributions and the
+// stencil weights are insensitive (~2e-7) and are left to FMA contraction.
+// The waveform phase and the position update are also rounded step by step.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -40,6 +45,15 @@ struct JfMaterials {
 };
 
 __device__ __forceinline__ int jf_mat_slot(int mt) { return (mt >= 0 && mt <= 3) ? mt : 4; }
+
+// separately rounded FP32 operations (never fused)
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+// a*b + c*d with each product and the sum rounded on its own
+__device__ __forceinline__ float rdot2(float a, float b, float c, float d) {
+  return __fadd_rn(__fmul_rn(a, b), __fmul_rn(c, d));
+}
 
 // Activation of the 2-phase waveform (mpm_sim.py:173-180): Python float
 // modulo as a - b*floor(a/b), half-cosine arch while phase < contraction.
@@ -79,36 +93,39 @@ __host__ __device__ inline float jf_activation(float freq, float contraction, fl
 // rotation of S unless |S01| < 1e-5, singular values ordered s1 >= s2 with
 // the matching V, U = R V.  Matrices row-major in float4 (00, 01, 10, 11).
 __device__ __forceinline__ void jf_svd2(float4 A, float4& U, float2& sig, float4& V) {
-  float x = A.x + A.w;
-  float y = A.z - A.y;
-  float scale = 1.0f / sqrtf(x * x + y * y);
-  float c = x * scale;
-  float s = y * scale;
-  float ms = -s;
-  float S00 = c * A.x + s * A.z;
-  float S01 = c * A.y + s * A.w;
-  float S11 = ms * A.y + c * A.w;
+  const float x = radd(A.x, A.w);
+  const float y = rsub(A.z, A.y);
+  const float scale = 1.0f / sqrtf(radd(rmul(x, x), rmul(y, y)));
+  const float c = rmul(x, scale);
+  const float s = rmul(y, scale);
+  const float ms = -s;
+  const float S00 = rdot2(c, A.x, s, A.z);
+  const float S01 = rdot2(c, A.y, s, A.w);
+  const float S11 = rdot2(ms, A.y, c, A.w);
   float cc, ss, s1, s2;
   if (fabsf(S01) < 1e-5f) {
     cc = 1.0f; ss = 0.0f;
     s1 = S00; s2 = S11;
   } else {
-    float tao = 0.5f * (S00 - S11);
-    float w = sqrtf(tao * tao + S01 * S01);
-    float t = tao > 0.0f ? S01 / (tao + w) : S01 / (tao - w);
-    cc = 1.0f / sqrtf(t * t + 1.0f);
-    ss = (-t) * cc;
-    s1 = (cc * cc * S00 - 2.0f * cc * ss * S01) + ss * ss * S11;
-    s2 = (ss * ss * S00 + 2.0f * cc * ss * S01) + cc * cc * S11;
+    const float tao = rmul(0.5f, rsub(S00, S11));
+    const float w = sqrtf(radd(rmul(tao, tao), rmul(S01, S01)));
+    const float t = tao > 0.0f ? S01 / radd(tao, w) : S01 / rsub(tao, w);
+    cc = 1.0f / sqrtf(radd(rmul(t, t), 1.0f));
+    ss = rmul(-t, cc);
+    const float cc2 = rmul(cc, cc), ss2 = rmul(ss, ss);
+    const float cs2 = rmul(rmul(2.0f, cc), ss);
+    s1 = radd(rsub(rmul(cc2, S00), rmul(cs2, S01)), rmul(ss2, S11));
+    s2 = radd(radd(rmul(ss2, S00), rmul(cs2, S01)), rmul(cc2, S11));
   }
   float V00, V01, V10, V11;
   if (s1 < s2) {
-    float tmp = s1; s1 = s2; s2 = tmp;
+    const float tmp = s1; s1 = s2; s2 = tmp;
     V00 = -ss; V01 = cc; V10 = -cc; V11 = -ss;
   } else {
     V00 = cc; V01 = ss; V10 = -ss; V11 = cc;
   }
-  U = make_float4(c * V00 + ms * V10, c * V01 + ms * V11, s * V00 + c * V10, s * V01 + c * V11);
+  U = make_float4(rdot2(c, V00, ms, V10), rdot2(c, V01, ms, V11), rdot2(s, V00, c, V10),
+                  rdot2(s, V01, c, V11));
   V = make_float4(V00, V01, V10, V11);
   sig = make_float2(s1, s2);
 }
@@ -159,12 +176,10 @@ __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMateria
                                                 JfScatter& o) {
   const float dt = I.dt;
   {
-    float A00 = 1.0f + dt * C.x, A01 = dt * C.y, A10 = dt * C.z, A11 = 1.0f + dt * C.w;
-    float F00 = A00 * F.x + A01 * F.z;
-    float F01 = A00 * F.y + A01 * F.w;
-    float F10 = A10 * F.x + A11 * F.z;
-    float F11 = A10 * F.y + A11 * F.w;
-    F = make_float4(F00, F01, F10, F11);
+    const float A00 = radd(1.0f, rmul(dt, C.x)), A01 = rmul(dt, C.y);
+    const float A10 = rmul(dt, C.z), A11 = radd(1.0f, rmul(dt, C.w));
+    F = make_float4(rdot2(A00, F.x, A01, F.z), rdot2(A00, F.y, A01, F.w), rdot2(A10, F.x, A11, F.z),
+                    rdot2(A10, F.y, A11, F.w));
   }
   // constant-index selects keep the table in registers (no local-memory copy)
   const int ms = jf_mat_slot(mt);
@@ -173,56 +188,56 @@ __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMateria
   const float la = ms == 0 ? mats.la[0] : ms == 1 ? mats.la[1] : ms == 2 ? mats.la[2]
                  : ms == 3 ? mats.la[3] : mats.la[4];
   float mass = I.p_mass;
-  if (mt == 2) mass = mass * pdens;
+  if (mt == 2) mass = rmul(mass, pdens);
 
   float4 U, V;
   float2 sig;
   jf_svd2(F, U, sig, V);
   sig.x = fmaxf(sig.x, 1e-6f);
   sig.y = fmaxf(sig.y, 1e-6f);
-  float J;
   if (mt == 2) {
-    float n0 = fminf(fmaxf(sig.x, 0.995f), 1.005f);
-    float n1 = fminf(fmaxf(sig.y, 0.995f), 1.005f);
-    Jp = Jp * (sig.x / n0);
-    Jp = Jp * (sig.y / n1);
+    const float n0 = fminf(fmaxf(sig.x, 0.995f), 1.005f);
+    const float n1 = fminf(fmaxf(sig.y, 0.995f), 1.005f);
+    Jp = rmul(Jp, sig.x / n0);
+    Jp = rmul(Jp, sig.y / n1);
     sig = make_float2(n0, n1);
   }
-  J = sig.x * sig.y;
+  const float J = rmul(sig.x, sig.y);
   if (mt == 0) {
-    float sj = sqrtf(J);
+    const float sj = sqrtf(J);
     F = make_float4(sj, 0.0f, 0.0f, sj);
   } else if (mt == 2) {
-    float US00 = U.x * sig.x, US01 = U.y * sig.y, US10 = U.z * sig.x, US11 = U.w * sig.y;
-    F = make_float4(US00 * V.x + US01 * V.y, US00 * V.z + US01 * V.w,
-                    US10 * V.x + US11 * V.y, US10 * V.z + US11 * V.w);
+    const float US00 = rmul(U.x, sig.x), US01 = rmul(U.y, sig.y);
+    const float US10 = rmul(U.z, sig.x), US11 = rmul(U.w, sig.y);
+    F = make_float4(rdot2(US00, V.x, US01, V.y), rdot2(US00, V.z, US01, V.w),
+                    rdot2(US10, V.x, US11, V.y), rdot2(US10, V.z, US11, V.w));
   }
-  float R00 = U.x * V.x + U.y * V.y;
-  float R01 = U.x * V.z + U.y * V.w;
-  float R10 = U.z * V.x + U.w * V.y;
-  float R11 = U.z * V.z + U.w * V.w;
-  float twomu = 2.0f * mu;
-  float E00 = twomu * (F.x - R00), E01 = twomu * (F.y - R01);
-  float E10 = twomu * (F.z - R10), E11 = twomu * (F.w - R11);
-  float diag = la * J * (J - 1.0f);
-  float s00 = (E00 * F.x + E01 * F.y) + diag;
-  float s01 = E00 * F.z + E01 * F.w;
-  float s10 = E10 * F.x + E11 * F.y;
-  float s11 = (E10 * F.z + E11 * F.w) + diag;
+  const float R00 = rdot2(U.x, V.x, U.y, V.y);
+  const float R01 = rdot2(U.x, V.z, U.y, V.w);
+  const float R10 = rdot2(U.z, V.x, U.w, V.y);
+  const float R11 = rdot2(U.z, V.z, U.w, V.w);
+  const float twomu = rmul(2.0f, mu);
+  const float E00 = rmul(twomu, rsub(F.x, R00)), E01 = rmul(twomu, rsub(F.y, R01));
+  const float E10 = rmul(twomu, rsub(F.z, R10)), E11 = rmul(twomu, rsub(F.w, R11));
+  const float diag = rmul(rmul(la, J), rsub(J, 1.0f));
+  float s00 = radd(rdot2(E00, F.x, E01, F.y), diag);
+  float s01 = rdot2(E00, F.z, E01, F.w);
+  float s10 = rdot2(E10, F.x, E11, F.y);
+  float s11 = radd(rdot2(E10, F.z, E11, F.w), diag);
   if (mt == 3) {
-    s00 = s00 + fiber.x * fiber.x * pressure * J;
-    s01 = s01 + fiber.x * fiber.y * pressure * J;
-    s10 = s10 + fiber.y * fiber.x * pressure * J;
-    s11 = s11 + fiber.y * fiber.y * pressure * J;
+    s00 = radd(s00, rmul(rmul(rmul(fiber.x, fiber.x), pressure), J));
+    s01 = radd(s01, rmul(rmul(rmul(fiber.x, fiber.y), pressure), J));
+    s10 = radd(s10, rmul(rmul(rmul(fiber.y, fiber.x), pressure), J));
+    s11 = radd(s11, rmul(rmul(rmul(fiber.y, fiber.y), pressure), J));
   }
   const float k = I.stress_scale;
   o.mass = mass;
-  o.af00 = k * s00 + mass * C.x;
-  o.af01 = k * s01 + mass * C.y;
-  o.af10 = k * s10 + mass * C.z;
-  o.af11 = k * s11 + mass * C.w;
-  o.mv0 = mass * v.x;
-  o.mv1 = mass * v.y;
+  o.af00 = rdot2(k, s00, mass, C.x);
+  o.af01 = rdot2(k, s01, mass, C.y);
+  o.af10 = rdot2(k, s10, mass, C.z);
+  o.af11 = rdot2(k, s11, mass, C.w);
+  o.mv0 = rmul(mass, v.x);
+  o.mv1 = rmul(mass, v.y);
 }
 
 // Contribution of a particle to stencil node (i, j), i, j in 0..2

@@ -58,6 +58,7 @@ struct jf_engine {
   int32_t* d_err = nullptr;        // per-instance non-finite flags
   float* d_stage = nullptr;        // host <-> device staging (max_slots * 8 floats)
   int32_t* d_stage_i = nullptr;    // staging for ints (max_slots * 2)
+  unsigned long long* d_path = nullptr;  // batched path counters (see jf_path_counts)
 
   bool sorted = false;             // batched path: particle order valid for the current state
   float t = 0.0f;                  // sim_time (FP32 running sum, mpm_sim.py:340)

@@ -101,6 +101,14 @@ class Engine:
         return {"step_ms": sm.value, "step_launches": sl.value, "sort_ms": om.value,
                 "sort_launches": ol.value}
 
+    def path_counts(self, reset: bool = False) -> dict:
+        """Batched path counters: register-block scatters, per-particle scatters,
+        gathers outside the CTA window."""
+        out = np.zeros(3, np.int64)
+        self._check(self._lib.jf_path_counts(self._h, _ptr(out), 1 if reset else 0))
+        return {"register_scatters": int(out[0]), "atomic_scatters": int(out[1]),
+                "remote_gathers": int(out[2])}
+
     def set_stream(self, stream) -> None:
         """Queue work on ``stream`` (a cudaStream_t as int, or a torch.cuda.Stream)."""
         handle = getattr(stream, "cuda_stream", stream)

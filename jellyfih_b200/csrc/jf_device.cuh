@@ -102,21 +102,23 @@ __device__ __forceinline__ void jf_svd2(float4 A, float4& U, float2& sig, float4
   const float S00 = rdot2(c, A.x, s, A.z);
   const float S01 = rdot2(c, A.y, s, A.w);
   const float S11 = rdot2(ms, A.y, c, A.w);
-  float cc, ss, s1, s2;
-  if (fabsf(S01) < 1e-5f) {
-    cc = 1.0f; ss = 0.0f;
-    s1 = S00; s2 = S11;
-  } else {
-    const float tao = rmul(0.5f, rsub(S00, S11));
-    const float w = sqrtf(radd(rmul(tao, tao), rmul(S01, S01)));
-    const float t = tao > 0.0f ? S01 / radd(tao, w) : S01 / rsub(tao, w);
-    cc = 1.0f / sqrtf(radd(rmul(t, t), 1.0f));
-    ss = rmul(-t, cc);
-    const float cc2 = rmul(cc, cc), ss2 = rmul(ss, ss);
-    const float cs2 = rmul(rmul(2.0f, cc), ss);
-    s1 = radd(rsub(rmul(cc2, S00), rmul(cs2, S01)), rmul(ss2, S11));
-    s2 = radd(radd(rmul(ss2, S00), rmul(cs2, S01)), rmul(cc2, S11));
-  }
+  // Both branches of the reference's |S01| < 1e-5 test are evaluated and the
+  // result selected, so lanes of a warp do not diverge; the selected values
+  // are those of the taken branch (the other one may be NaN and is dropped).
+  const float tao = rmul(0.5f, rsub(S00, S11));
+  const float w = sqrtf(radd(rmul(tao, tao), rmul(S01, S01)));
+  const float t = S01 / (tao > 0.0f ? radd(tao, w) : rsub(tao, w));
+  const float jc = 1.0f / sqrtf(radd(rmul(t, t), 1.0f));
+  const float js = rmul(-t, jc);
+  const float cc2 = rmul(jc, jc), ss2 = rmul(js, js);
+  const float cs2 = rmul(rmul(2.0f, jc), js);
+  const float j1 = radd(rsub(rmul(cc2, S00), rmul(cs2, S01)), rmul(ss2, S11));
+  const float j2 = radd(radd(rmul(ss2, S00), rmul(cs2, S01)), rmul(cc2, S11));
+  const bool diagonal = fabsf(S01) < 1e-5f;
+  const float cc = diagonal ? 1.0f : jc;
+  const float ss = diagonal ? 0.0f : js;
+  float s1 = diagonal ? S00 : j1;
+  float s2 = diagonal ? S11 : j2;
   float V00, V01, V10, V11;
   if (s1 < s2) {
     const float tmp = s1; s1 = s2; s2 = tmp;

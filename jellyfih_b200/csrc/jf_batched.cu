@@ -114,19 +114,39 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
 }
 
 // Adds a particle's 3x3 stencil into the lane's 4x4 node block, shifted by
-// (DI, DJ) = stencil base - (cell - 1).
-template <int DI, int DJ>
+// (di, dj) = stencil base - (cell - 1), both 0 or 1.  Branch-free: the
+// weights are shifted into 4-wide vectors with zeros outside the stencil, so
+// lanes with different shifts run the same instructions.  Contributions are
+// formed separably, weight_x * (m v + A (x_i - x_p)) per column and then
+// weight_y per row, a re-association of mpm_sim.py:256-271 that moves results
+// by rounding only.
 __device__ __forceinline__ void accumulate_block(float* acc, const JfInst& I, const JfStencil& st,
-                                                 const JfScatter& sc) {
+                                                 const JfScatter& sc, int di, int dj) {
+  const bool sx = di != 0, sy = dj != 0;
+  const float wx4[4] = {sx ? 0.0f : st.wx0, sx ? st.wx0 : st.wx1, sx ? st.wx1 : st.wx2, sx ? st.wx2 : 0.0f};
+  const float wy4[4] = {sy ? 0.0f : st.wy0, sy ? st.wy0 : st.wy1, sy ? st.wy1 : st.wy2, sy ? st.wy2 : 0.0f};
+  // node offsets from the particle: (I - di - fx0) dx; di + fx0 is exact
+  const float ex = (float)di + st.fx0, ey = (float)dj + st.fx1;
+  float P[4], Q0[4], Q1[4], Pm[4];
 #pragma unroll
-  for (int j = 0; j < 3; ++j) {
+  for (int i = 0; i < 4; ++i) {
+    const float d0 = ((float)i - ex) * I.dx;
+    P[i] = wx4[i];
+    Q0[i] = wx4[i] * (sc.mv0 + sc.af00 * d0);
+    Q1[i] = wx4[i] * (sc.mv1 + sc.af10 * d0);
+    Pm[i] = wx4[i] * sc.mass;
+  }
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const float3 c = jf_node_contrib(I, st, sc, i, j);
-      const int q = ((j + DJ) * 4 + (i + DI)) * 3;
-      acc[q + 0] += c.x;
-      acc[q + 1] += c.y;
-      acc[q + 2] += c.z;
+  for (int j = 0; j < 4; ++j) {
+    const float d1 = ((float)j - ey) * I.dx;
+    const float r0 = sc.af01 * d1, r1 = sc.af11 * d1;
+    const float wj = wy4[j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int q = (j * 4 + i) * 3;
+      acc[q + 0] += wj * (Q0[i] + P[i] * r0);
+      acc[q + 1] += wj * (Q1[i] + P[i] * r1);
+      acc[q + 2] += wj * Pm[i];
     }
   }
 }
@@ -332,14 +352,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
             const bool in_block = (unsigned)di < 2u && (unsigned)dj < 2u;
             n_fast += in_block ? 1u : 0u;
             n_generic += in_block ? 0u : 1u;
-            if (di == 0 && dj == 0) {
-              accumulate_block<0, 0>(acc, I, st, sc);
-            } else if (di == 1 && dj == 0) {
-              accumulate_block<1, 0>(acc, I, st, sc);
-            } else if (di == 0 && dj == 1) {
-              accumulate_block<0, 1>(acc, I, st, sc);
-            } else if (di == 1 && dj == 1) {
-              accumulate_block<1, 1>(acc, I, st, sc);
+            if (in_block) {
+              accumulate_block(acc, I, st, sc, di, dj);
             } else {
               scatter_particle(w, cluster, I, st, sc);
             }

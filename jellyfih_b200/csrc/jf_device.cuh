@@ -277,29 +277,40 @@ __device__ __forceinline__ float2 jf_grid_node(const JfInst& I, int i, int j, fl
 
 // APIC gather of G2P (mpm_sim.py:317-327) for a particle whose stencil is in
 // range: new v and C from the updated grid.  `gather(i, j)` returns the
-// updated velocity of stencil node (bx + i, by + j), i, j in 0..2.
+// updated velocity of stencil node (bx + i, by + j), i, j in 0..2.  The sums
+// are formed row by row (sum over i, then weighted by the y weight), a
+// re-association of the reference's node-by-node sum that moves results by
+// rounding only.
 template <class Gather>
 __device__ __forceinline__ void jf_g2p_apic(const JfInst& I, const JfStencil& st, float2& v, float4& C,
                                             Gather gather) {
+  const float wx[3] = {st.wx0, st.wx1, st.wx2};
+  const float wy[3] = {st.wy0, st.wy1, st.wy2};
+  float wxd[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) wxd[i] = wx[i] * ((float)i - st.fx0);
   float nv0 = 0.f, nv1 = 0.f, c00 = 0.f, c01 = 0.f, c10 = 0.f, c11 = 0.f;
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
+  for (int j = 0; j < 3; ++j) {
+    float sx = 0.f, sy = 0.f, tx = 0.f, ty = 0.f;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      float d0 = (float)i - st.fx0, d1 = (float)j - st.fx1;
-      float2 g = gather(i, j);
-      float weight = jf_w(st, 0, i) * jf_w(st, 1, j);
-      nv0 = nv0 + weight * g.x;
-      nv1 = nv1 + weight * g.y;
-      float k = I.c4 * weight;
-      c00 = c00 + k * (g.x * d0);
-      c01 = c01 + k * (g.x * d1);
-      c10 = c10 + k * (g.y * d0);
-      c11 = c11 + k * (g.y * d1);
+    for (int i = 0; i < 3; ++i) {
+      const float2 g = gather(i, j);
+      sx += wx[i] * g.x;
+      sy += wx[i] * g.y;
+      tx += wxd[i] * g.x;
+      ty += wxd[i] * g.y;
     }
+    const float wyd = wy[j] * ((float)j - st.fx1);
+    nv0 += wy[j] * sx;
+    nv1 += wy[j] * sy;
+    c00 += wy[j] * tx;
+    c01 += wyd * sx;
+    c10 += wy[j] * ty;
+    c11 += wyd * sy;
   }
   v = make_float2(nv0, nv1);
-  C = make_float4(c00, c01, c10, c11);
+  C = make_float4(I.c4 * c00, I.c4 * c01, I.c4 * c10, I.c4 * c11);
 }
 
 // Gravity, advection and the wall clamp of every live particle

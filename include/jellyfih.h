@@ -60,6 +60,8 @@ typedef struct {
  * contraction 0.2, frequency multiplier 1.0, payload density 2.5). */
 int jf_create(const jf_config* cfg, jf_engine** out);
 int jf_destroy(jf_engine* e);
+/* Message of the engine's last failure; with e == NULL, of the last failed
+ * call made without a handle (jf_create, jf_substep_noalloc). */
 const char* jf_last_error(const jf_engine* e);
 const char* jf_version(void);
 
@@ -134,6 +136,31 @@ int jf_clear_error_flags(jf_engine* e);
  * atomics (drifted or out-of-range particles), out[2] G2P gathers outside the
  * CTA's shared-memory window.  All zero on the plain path. */
 int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset);
+
+/* Largest grid, in nodes (n_grid * n_grid_y), jf_substep_noalloc accepts. */
+#define JF_NOALLOC_MAX_NODES 32768
+
+/* One substep of one instance that allocates no device memory.
+ *
+ * No counterpart in the reference: it serves callers that cannot call
+ * cudaMalloc when they step (allocators or memory pools that must not grow,
+ * host callbacks, embedders that own all device memory).  The caller passes
+ * device pointers in the reference's layouts -- x, v, fiber [n][2]; C, F
+ * [n][2][2] row-major; material, Jp, glow [n] -- and advances sim_time by dt
+ * itself; fiber NULL means (0, 1), glow NULL skips the render-only glow.
+ * x, v, fiber must be 8-byte and C, F 16-byte aligned.  The grid scratch is a
+ * file-scope device array of JF_NOALLOC_MAX_NODES float4 nodes (512 KiB) that
+ * every GPU loading the library holds until exit; larger grids are rejected
+ * with JF_ERR_UNSUPPORTED.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) with that device current, so make that
+ * first call before any stream capture.  All calls share the array and each
+ * call clears the nodes it uses; calls that overlap on the GPU race.  Work is
+ * queued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+int jf_substep_noalloc(int32_t n, int32_t n_grid, int32_t n_grid_y, float domain_height, double dt,
+                       float sim_time, float actuation, float contraction, float freq,
+                       float payload_density, float* x, float* v, float* C, float* F,
+                       const int32_t* material, float* Jp, float* glow, const float* fiber,
+                       void* stream);
 
 /* Number of kernels this engine has launched. */
 int64_t jf_kernel_launches(const jf_engine* e);

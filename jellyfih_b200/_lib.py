@@ -59,6 +59,10 @@ EXPORTS = {
     "jf_error_flags": (ctypes.c_int, [_E, _P]),
     "jf_clear_error_flags": (ctypes.c_int, [_E]),
     "jf_kernel_launches": (ctypes.c_int64, [_E]),
+    "jf_substep_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_float, ctypes.c_double, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                          ctypes.c_float] + [_P] * 9),
     "jf_path_counts": (ctypes.c_int, [_E, _P, ctypes.c_int32]),
     "jf_set_kernel_timing": (ctypes.c_int, [_E, ctypes.c_int32]),
     "jf_kernel_timing": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_double),

@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -15,7 +16,8 @@ int jf_batched_max_active_clusters(jf_engine* e, int cluster, int* out);
 
 namespace {
 
-std::string g_create_err;  // message of the last failed jf_create
+std::mutex g_err_mu;
+std::string g_create_err;  // message of the last failed call without a handle
 
 constexpr int kHaloRows = 4;  // batched window rows beyond the band (1 below, 3 above)
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -176,6 +178,11 @@ cudaError_t collect_timing(jf_engine* e) {
 
 }  // namespace
 
+void jf_set_global_error(const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_create_err = msg;
+}
+
 static cudaEvent_t pool_event(jf_engine* e) {
   if (!e->event_pool.empty()) {
     cudaEvent_t ev = e->event_pool.back();
@@ -204,17 +211,21 @@ extern "C" {
 
 const char* jf_version(void) { return "jellyfih-b200 0.1"; }
 
-const char* jf_last_error(const jf_engine* e) { return e ? e->err.c_str() : g_create_err.c_str(); }
+const char* jf_last_error(const jf_engine* e) {
+  if (e) return e->err.c_str();
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return g_create_err.c_str();
+}
 
 int jf_create(const jf_config* cfg, jf_engine** out) {
   if (!out) return JF_ERR_INVALID;
   *out = nullptr;
   if (!cfg || cfg->n_instances <= 0 || !cfg->instances) {
-    g_create_err = "config needs n_instances > 0 and an instance table";
+    jf_set_global_error("config needs n_instances > 0 and an instance table");
     return JF_ERR_INVALID;
   }
   if (cfg->path != JF_PATH_PLAIN && cfg->path != JF_PATH_BATCHED) {
-    g_create_err = "unknown path";
+    jf_set_global_error("unknown path");
     return JF_ERR_INVALID;
   }
   jf_engine* e = new jf_engine();
@@ -226,7 +237,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 16;
   e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
   auto bail = [&](int code, const std::string& msg) {
-    g_create_err = msg;
+    jf_set_global_error(msg);
     jf_destroy(e);
     return code;
   };

@@ -82,6 +82,10 @@ struct JfTimed {
   ~JfTimed();
 };
 
+// Message of the last failed call made without an engine handle
+// (jf_create, jf_substep_noalloc); returned by jf_last_error(NULL).
+void jf_set_global_error(const std::string& msg);
+
 // Lame parameters by material id (mpm_sim.py:25-48), passed to kernels by value.
 JfMaterials jf_materials();
 

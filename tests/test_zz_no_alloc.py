@@ -1,0 +1,99 @@
+"""jf_substep_noalloc: the allocation-free substep, checked against the engine.
+
+The entry point serves callers that cannot allocate device memory while
+stepping (a pool or allocator that must not grow, host callbacks, embedders
+owning all device memory); its grid scratch is a fixed device array inside the
+library.  Here it is called twice in a row through the C ABI on device arrays
+allocated up front, starting from a state the engine evolved for 300
+substeps, and each call's result is compared with one plain-engine substep
+(jf_step) from the same input, within the single-substep tolerance the parity
+tests use (1e-5 of the field max-norm).  Before the second call the engine is
+given the first call's output, so both comparisons start from identical
+states: near-incompressible water (lambda = 1e5) amplifies a relative error
+in J by about 1/(J - 1) ~ 1e3 per substep, so two substeps from states that
+already differ by summation-order noise diverge by ~6e-4 (measured with the
+CPU oracle).  A scratch grid that was not cleared between the calls would
+still show up as a gross mismatch.  The file is named to be collected last.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+FIELD_RTOL = 1e-5  # one substep from identical inputs: atomic summation order only
+
+
+def _norm_close(a, b, rtol, what):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.abs(b).max()
+    err = np.abs(a - b).max()
+    assert err <= rtol * max(scale, 1e-30), f"{what}: max|diff| {err:.3e} > {rtol} * {scale:.3e}"
+
+
+def test_noalloc_matches_engine_on_two_calls():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import Engine, InstanceSpec, _lib, build, tank
+    build.build()
+    lib = _lib.load()
+    torch.cuda.set_device(0)
+
+    genome = tank.uniform_genomes(1, 77)[0]
+    n = 80000
+    pos, mat, fib, st = tank.fill_tank(genome, n, jitter=0.25, seed=77)
+    contraction, freq = tank.timing_params(genome)
+    live = mat >= 0
+    act, pdens, dt = 650.0, 3.0, 2e-5
+
+    # a naturally evolved state: 300 substeps of the engine from the loaded tank
+    eng = Engine([InstanceSpec(n)], path="plain", glow=True)
+    eng.load(0, pos, mat, fib)
+    eng.set_params(actuation=[act], contraction=[contraction], freq=[freq], payload_density=[pdens])
+    eng.time = 0.0
+    eng.step(300)
+    s0 = eng.read(0)
+    t0 = eng.time
+
+    dev = torch.device("cuda", 0)
+    bufs = {k: torch.from_numpy(np.ascontiguousarray(s0[k])).to(dev)
+            for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber")}
+    stream = torch.cuda.current_stream(dev)
+    t = t0
+    for call in range(2):
+        if call > 0:  # both paths start this call from the first call's output
+            eng.write(0, x=got["x"], v=got["v"], C=got["C"], F=got["F"], Jp=got["Jp"],
+                      glow=got["glow"])
+        rc = lib.jf_substep_noalloc(
+            n, 128, 128, 1.0, dt, float(t), act, contraction, freq, pdens,
+            *[bufs[k].data_ptr() for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber")],
+            stream.cuda_stream)
+        assert rc == 0, lib.jf_last_error(None)
+        t = np.float32(t + np.float32(dt))
+        eng.step(1)
+        torch.cuda.synchronize()
+        ref = eng.read(0)
+        got = {k: bufs[k].cpu().numpy() for k in ("x", "v", "C", "F", "Jp", "glow")}
+        tol_x = 4 * np.spacing(np.float32(1.0))
+        assert np.abs(got["x"][live].astype(np.float64) - ref["x"][live]).max() <= tol_x, call
+        for k in ("v", "C", "F", "Jp", "glow"):
+            _norm_close(got[k][live], ref[k][live], FIELD_RTOL, f"call {call} {k}")
+        assert np.array_equal(got["x"][~live], ref["x"][~live])
+    assert eng.time == t
+    eng.close()
+
+
+def test_noalloc_rejects_oversized_grid_and_bad_arguments():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import _lib
+    lib = _lib.load()
+    null = [None] * 9
+    assert lib.jf_substep_noalloc(0, 256, 256, 2.0, 2e-5, 0.0, 500.0, 0.2, 1.0, 2.5, *null) == \
+        _lib.JF_ERR_UNSUPPORTED
+    assert b"scratch array" in lib.jf_last_error(None)
+    assert lib.jf_substep_noalloc(-1, 128, 128, 1.0, 2e-5, 0.0, 500.0, 0.2, 1.0, 2.5, *null) == \
+        _lib.JF_ERR_INVALID
+    assert lib.jf_substep_noalloc(10, 128, 128, 1.0, 2e-5, 0.0, 500.0, 0.2, 1.0, 2.5, *null) == \
+        _lib.JF_ERR_INVALID

@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--substeps", type=int, default=1000, help="substeps per bench step")
     ap.add_argument("--instances", type=int, default=32, help="instances per GPU")
     ap.add_argument("--slots", type=int, default=80000)
-    ap.add_argument("--resort", type=int, default=16)
+    ap.add_argument("--resort", type=int, default=64)
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
     return ap.parse_args()

@@ -51,7 +51,7 @@ typedef struct {
   int32_t path;                         /* JF_PATH_* */
   uint32_t flags;                       /* JF_FLAG_* */
   int32_t device;                       /* CUDA device ordinal */
-  int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 16 */
+  int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 64 */
   int32_t block_threads;                /* batched: threads per CTA, 0 = 512 */
 } jf_config;
 

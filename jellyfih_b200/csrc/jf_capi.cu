@@ -234,7 +234,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   e->dt = cfg->dt > 0 ? cfg->dt : 2e-5;
   e->path = cfg->path;
   e->flags = cfg->flags;
-  e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 16;
+  e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 64;
   e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
   auto bail = [&](int code, const std::string& msg) {
     jf_set_global_error(msg);

@@ -46,7 +46,7 @@ class Engine:
     """
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
-                 glow: bool = False, device: int = 0, resort_interval: int = 16,
+                 glow: bool = False, device: int = 0, resort_interval: int = 64,
                  block_threads: int = 512):
         self._lib = L.load()
         self.instances = list(instances)

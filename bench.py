@@ -319,9 +319,8 @@ def run_ours(args):
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": res.nbytes + 2 * 6 * 8 * M,
                          "steps": e2e_steps, "api": "Engine.load + Engine.run_headless (C ABI)"}
         if world > 1:
-            allres = [torch.zeros((M, 5), dtype=torch.float64, device="cuda") for _ in range(world)]
-            dist.all_gather(allres, torch.from_numpy(res).cuda())
-            extras["e2e"]["gathered_results"] = int(sum(r.shape[0] for r in allres))
+            from jellyfih_b200.shard import gather_rows
+            extras["e2e"]["gathered_results"] = int(gather_rows(res).shape[0])
 
         # plain per-instance launch path on the same inputs (BASELINE: batched vs plain)
         plain = Engine([spec] * M, path="plain", device=local)

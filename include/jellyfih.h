@@ -112,6 +112,18 @@ int jf_stats_raw(jf_engine* e, double* out);
  * final_y, final_x, valid] with valid = final_y >= 0.01. */
 int jf_run_headless(jf_engine* e, int64_t steps, double* out);
 
+/* Fitness of every instance from run_headless rows, computed on the GPU in
+ * FP64 (evolve.py:90-124 compute_fitness): invalid when valid == 0 or
+ * muscle_counts[m] < 200; displacement = min(final_y, domain_height - 0.07)
+ * - init_y; mode 0 (efficiency) scores -displacement / sqrt(muscle_counts[m]
+ * * clip(contraction[m], 0.05, 0.60) / 500) (contraction NULL: 0.20), mode 1
+ * (displacement) scores -displacement; invalid instances get the worst valid
+ * score + 1, or 100 when none is valid.  results: host [n_instances][5],
+ * muscle_counts, contraction (gene 9, unclipped): host [n_instances], out:
+ * host [n_instances]. */
+int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts,
+               const double* contraction, int32_t mode, double* out);
+
 /* Particle fields of instance m in slot order (field.to_numpy()); any
  * pointer may be NULL.  x, v, fiber: [n_slots][2]; C, F: [n_slots][4]. */
 int jf_read_particles(jf_engine* e, int32_t m, float* x, float* v, float* C, float* F,

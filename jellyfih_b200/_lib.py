@@ -53,6 +53,7 @@ EXPORTS = {
     "jf_stats_any": (ctypes.c_int, [_E, _P]),
     "jf_stats_raw": (ctypes.c_int, [_E, _P]),
     "jf_run_headless": (ctypes.c_int, [_E, ctypes.c_int64, _P]),
+    "jf_fitness": (ctypes.c_int, [_E, _P, _P, _P, ctypes.c_int32, _P]),
     "jf_read_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "jf_write_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P]),
     "jf_read_grid": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P]),

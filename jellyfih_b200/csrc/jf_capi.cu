@@ -287,6 +287,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     I.c4 = (float)(4 * nx);
     I.dtg = (float)(e->dt * 10.0);
     I.y_hi = (float)((double)d.domain_height - 0.001);
+    I.domain_h = (double)d.domain_height;
     e->inst.push_back(I);
     JfParams P = {500.0f, 0.20f, 1.0f, 2.5f};  // mpm_sim.py:143-149
     e->params.push_back(P);
@@ -315,7 +316,10 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
       (err = alloc(&e->d_stats, 6 * (size_t)e->M)) != cudaSuccess ||
       (err = alloc(&e->d_err, e->M)) != cudaSuccess ||
       (err = alloc(&e->d_stage, 8 * (size_t)e->max_slots)) != cudaSuccess ||
-      (err = alloc(&e->d_stage_i, 2 * (size_t)e->max_slots)) != cudaSuccess)
+      (err = alloc(&e->d_stage_i, 2 * (size_t)e->max_slots)) != cudaSuccess ||
+      (err = alloc(&e->d_fit, 6 * (size_t)e->M)) != cudaSuccess ||
+      (err = alloc(&e->d_fit_f, e->M)) != cudaSuccess ||
+      (err = alloc(&e->d_fit_i, e->M)) != cudaSuccess)
     return bail(JF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
   if (e->path == JF_PATH_BATCHED) {
     if ((err = alloc_particles(e->q, p_off)) != cudaSuccess ||
@@ -361,6 +365,7 @@ int jf_destroy(jf_engine* e) {
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_band); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
+  cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i);
   for (auto& pr : e->step_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto& pr : e->sort_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto ev : e->event_pool) cudaEventDestroy(ev);
@@ -510,6 +515,27 @@ int jf_run_headless(jf_engine* e, int64_t steps, double* out) {
       o[4] = (b[0] < 0.01) ? 0.0 : 1.0;
     }
   }
+  return JF_OK;
+}
+
+int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts, const double* contraction,
+               int32_t mode, double* out) {
+  if (check_engine(e) || !results || !muscle_counts || !out) return JF_ERR_INVALID;
+  if (mode != 0 && mode != 1) return fail(e, JF_ERR_INVALID, "fitness mode must be 0 or 1");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const size_t M = (size_t)e->M;
+  double* d_rows = e->d_fit;       // 5M doubles
+  double* d_out = e->d_fit + 5 * M;  // M doubles
+  double* d_con = e->d_fit_f;      // M doubles
+  int32_t* d_mus = e->d_fit_i;     // M ints
+  JF_CK(cudaMemcpyAsync(d_rows, results, sizeof(double) * 5 * M, cudaMemcpyHostToDevice, e->stream), "fitness rows");
+  JF_CK(cudaMemcpyAsync(d_mus, muscle_counts, sizeof(int32_t) * M, cudaMemcpyHostToDevice, e->stream), "fitness counts");
+  if (contraction)
+    JF_CK(cudaMemcpyAsync(d_con, contraction, sizeof(double) * M, cudaMemcpyHostToDevice, e->stream), "fitness genes");
+  JF_CK(jf_fitness_launch(e, d_rows, d_mus, contraction ? d_con : nullptr, mode, d_out), "fitness kernel");
+  JF_CK(cudaMemcpyAsync(out, d_out, sizeof(double) * M, cudaMemcpyDeviceToHost, e->stream), "fitness read");
+  JF_CK(cudaStreamSynchronize(e->stream), "fitness sync");
   return JF_OK;
 }
 

@@ -27,6 +27,7 @@ struct JfInst {
   float c4;             // 4 * inv_dx (:326)
   float dtg;            // dt * gravity (:329)
   float y_hi;           // domain_height - 0.001 (:333)
+  double domain_h;      // domain_height as the caller gave it (fitness ceiling, evolve.py:101)
 };
 
 // Mutable per-instance waveform / material parameters (mpm_sim.py:116-149).

@@ -59,6 +59,9 @@ struct jf_engine {
   float* d_stage = nullptr;        // host <-> device staging (max_slots * 8 floats)
   int32_t* d_stage_i = nullptr;    // staging for ints (max_slots * 2)
   unsigned long long* d_path = nullptr;  // batched path counters (see jf_path_counts)
+  double* d_fit = nullptr;         // fitness staging: M x 5 rows + M scores
+  double* d_fit_f = nullptr;       // fitness staging: M contraction genes
+  int32_t* d_fit_i = nullptr;      // fitness staging: M muscle counts
 
   bool sorted = false;             // batched path: particle order valid for the current state
   float t = 0.0f;                  // sim_time (FP32 running sum, mpm_sim.py:340)
@@ -96,6 +99,10 @@ cudaError_t jf_plain_step(jf_engine* e, int64_t n_steps);
 cudaError_t jf_batched_step(jf_engine* e, int64_t n_steps);
 cudaError_t jf_batched_sort(jf_engine* e);
 size_t jf_batched_smem_bytes(const jf_engine* e);
+
+// Fitness of every instance from (M, 5) rows on the device (FP64).
+cudaError_t jf_fitness_launch(jf_engine* e, const double* d_rows, const int32_t* d_muscle,
+                              const double* d_contraction, int mode, double* d_out);
 
 // CoM sums of every instance into e->d_stats (M x 6 doubles).
 cudaError_t jf_stats_launch(jf_engine* e);

@@ -152,6 +152,7 @@ extern "C" int jf_substep_noalloc(int32_t n, int32_t n_grid, int32_t n_grid_y, f
   I.c4 = (float)(4.0 * n_grid);
   I.dtg = (float)(dt * 10.0);
   I.y_hi = (float)((double)domain_height - 0.001);
+  I.domain_h = (double)domain_height;
   const JfParams P = {actuation, contraction, freq, payload_density};
   const float pressure = actuation * jf_activation(freq, contraction, sim_time);
   cudaStream_t s = (cudaStream_t)stream;

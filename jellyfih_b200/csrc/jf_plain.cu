@@ -157,6 +157,60 @@ __global__ void glow_to_slot_kernel(JfInst I, const float* __restrict__ glow,
   out[slot[g]] = glow[g];
 }
 
+// Fitness of every instance (evolve.py:90-124) in FP64: one block, the
+// penalty for invalid instances is the block maximum of the valid scores + 1.
+__global__ void fitness_kernel(const JfInst* __restrict__ inst, int M, const double* __restrict__ rows,
+                               const int32_t* __restrict__ muscle, const double* __restrict__ contraction,
+                               int has_contraction, int mode, double* __restrict__ out) {
+  __shared__ double s_max[32];
+  __shared__ int s_any[32];
+  double best = -INFINITY;
+  int any = 0;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    const double* r = rows + 5 * (size_t)m;
+    const double valid = r[4];
+    double score = NAN;
+    if (!(valid == 0.0 || muscle[m] < 200)) {
+      const double cap = inst[m].domain_h - 0.07;
+      const double disp = (r[2] < cap ? r[2] : cap) - r[0];
+      if (mode == 1) {
+        score = -disp;
+      } else {
+        double frac = has_contraction ? contraction[m] : 0.20;
+        frac = frac < 0.05 ? 0.05 : (frac > 0.60 ? 0.60 : frac);
+        const double cost = sqrt((double)muscle[m] * frac / 500.0);
+        score = -disp / cost;
+      }
+      best = score > best ? score : best;
+      any = 1;
+    }
+    out[m] = score;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    best = fmax(best, __shfl_down_sync(0xffffffffu, best, off));
+    any |= __shfl_down_sync(0xffffffffu, any, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_max[threadIdx.x >> 5] = best;
+    s_any[threadIdx.x >> 5] = any;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = -INFINITY;
+    int a = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      b = s_max[w] > b ? s_max[w] : b;
+      a |= s_any[w];
+    }
+    s_max[0] = a ? b + 1.0 : 100.0;
+  }
+  __syncthreads();
+  const double penalty = s_max[0];
+  for (int m = threadIdx.x; m < M; m += blockDim.x)
+    if (isnan(out[m])) out[m] = penalty;
+}
+
 inline int blocks_for(int64_t n) { return (int)((n + kThreads - 1) / kThreads); }
 
 }  // namespace
@@ -204,6 +258,14 @@ cudaError_t jf_stats_launch(jf_engine* e) {
   if (blocks < 1) blocks = 1;
   stats_kernel<<<dim3(blocks, e->M), kThreads, 0, e->stream>>>(e->d_inst, e->p.xv, e->p.mat,
                                                                  e->d_stats);
+  e->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_fitness_launch(jf_engine* e, const double* d_rows, const int32_t* d_muscle,
+                              const double* d_contraction, int mode, double* d_out) {
+  fitness_kernel<<<1, 1024, 0, e->stream>>>(e->d_inst, e->M, d_rows, d_muscle, d_contraction,
+                                            d_contraction != nullptr, mode, d_out);
   e->launches += 1;
   return cudaGetLastError();
 }

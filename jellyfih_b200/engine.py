@@ -173,6 +173,17 @@ class Engine:
         self._check(self._lib.jf_run_headless(self._h, int(steps), _ptr(out)))
         return out
 
+    def fitness(self, results, muscle_counts, contraction=None, mode: str = "efficiency") -> np.ndarray:
+        """Per-instance fitness of run_headless rows, computed on the GPU in FP64
+        (evolve.py:90-124); lower is better, as CMA-ES minimises."""
+        rows = np.ascontiguousarray(results, dtype=np.float64).reshape(self.M, 5)
+        mus = np.ascontiguousarray(muscle_counts, dtype=np.int32).reshape(self.M)
+        con = None if contraction is None else np.ascontiguousarray(contraction, dtype=np.float64).reshape(self.M)
+        out = np.zeros(self.M, np.float64)
+        self._check(self._lib.jf_fitness(self._h, _ptr(rows), _ptr(mus), _ptr(con),
+                                         {"efficiency": 0, "displacement": 1}[mode], _ptr(out)))
+        return out
+
     def read(self, m: int) -> dict:
         n = self.instances[m].n_slots
         d = {"x": np.zeros((n, 2), np.float32), "v": np.zeros((n, 2), np.float32),

@@ -273,3 +273,32 @@ def test_mpm_sim_module_drop_in(monkeypatch):
     sim.substep()
     sim.engine().close()
     sys.modules.pop("jellyfih_b200.mpm_sim", None)
+
+
+def test_gpu_fitness_matches_host_restatement():
+    """Engine.fitness (FP64 kernel) against evolve.py's compute_fitness restated on the host."""
+    from jellyfih_b200 import InstanceSpec
+    from jellyfih_b200.fitness import compute_fitness
+    rng = np.random.default_rng(9)
+    M = 40
+    specs = [InstanceSpec(100, 128, 128 if m % 3 else 256, 1.0 if m % 3 else 2.0) for m in range(M)]
+    e = _engine(specs, "plain")
+    rows = np.zeros((M, 5))
+    rows[:, 0] = rng.uniform(0.3, 0.5, M)
+    rows[:, 2] = rows[:, 0] + rng.normal(0, 0.05, M)
+    rows[::7, 2] = 1.99                      # capped at domain_height - 0.07
+    rows[:, 4] = (rng.random(M) > 0.15).astype(float)
+    muscle = rng.integers(100, 900, M).astype(np.int32)
+    genes = rng.uniform(0.0, 0.8, M)
+    genomes = [np.r_[np.zeros(9), g, 1.0] for g in genes]
+    for mode in ("efficiency", "displacement"):
+        got = e.fitness(rows, muscle, genes, mode=mode)
+        ref = np.zeros(M)
+        for dh in (1.0, 2.0):  # each instance's own domain height
+            sel = np.array([(s.domain_height == dh) for s in specs])
+            r = compute_fitness(rows, muscle, genomes, domain_height=dh, mode=mode)
+            ref[sel] = np.asarray(r)[sel]
+        valid = (rows[:, 4] != 0) & (muscle >= 200)
+        np.testing.assert_allclose(got[valid], ref[valid], rtol=1e-15)
+        assert np.all(got[~valid] == got[valid].max() + 1.0)
+    e.close()

@@ -124,6 +124,21 @@ int jf_run_headless(jf_engine* e, int64_t steps, double* out);
 int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts,
                const double* contraction, int32_t mode, double* out);
 
+/* Differentiable rollout.  jf_grad_forward runs `steps` substeps from the
+ * current state with a deterministic P2G, checkpointing (x, v, C, F) every
+ * `checkpoint_every` substeps, and returns loss[m] = the displacement of the
+ * payload CoM height (jelly + muscle without payload) over the rollout, the
+ * quantity evolve.py's fitness is built from (evolve.py:101).  jf_grad_backward
+ * then returns d loss / d instance_actuation, instance_act_contraction and
+ * instance_freq (host arrays, NULL to skip; the refractory fraction is
+ * 1 - contraction, so its gradient is minus the contraction's), and
+ * jf_grad_positions the gradient w.r.t. instance m's initial positions in slot
+ * order ([n_slots][2]).  The reference engine has no gradients; this replaces
+ * nothing in it.  The engine is left at the rollout's final state. */
+int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss);
+int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, double* d_freq);
+int jf_grad_positions(jf_engine* e, int32_t m, float* dx0);
+
 /* Particle fields of instance m in slot order (field.to_numpy()); any
  * pointer may be NULL.  x, v, fiber: [n_slots][2]; C, F: [n_slots][4]. */
 int jf_read_particles(jf_engine* e, int32_t m, float* x, float* v, float* C, float* F,

@@ -360,6 +360,7 @@ int jf_destroy(jf_engine* e) {
   if (!e) return JF_ERR_INVALID;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  jf_grad_free(e);
   free_particles(e->p);
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
@@ -536,6 +537,76 @@ int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts
   JF_CK(jf_fitness_launch(e, d_rows, d_mus, contraction ? d_con : nullptr, mode, d_out), "fitness kernel");
   JF_CK(cudaMemcpyAsync(out, d_out, sizeof(double) * M, cudaMemcpyDeviceToHost, e->stream), "fitness read");
   JF_CK(cudaStreamSynchronize(e->stream), "fitness sync");
+  return JF_OK;
+}
+
+int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (steps <= 0 || checkpoint_every <= 0) return fail(e, JF_ERR_INVALID, "steps and checkpoint_every must be > 0");
+  int rc = set_device(e);
+  if (rc) return rc;
+  if ((rc = upload_params(e))) return rc;
+  std::vector<double> raw(6 * (size_t)e->M);
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  JF_CK(cudaMemcpyAsync(raw.data(), e->d_stats, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, e->stream),
+        "read stats");
+  JF_CK(cudaStreamSynchronize(e->stream), "stats sync");
+  std::vector<int32_t> body(e->M);
+  std::vector<double> inv_n(e->M), init(e->M);
+  for (int m = 0; m < e->M; ++m) {
+    const double* r = &raw[6 * (size_t)m];
+    body[m] = r[1] == 0 ? 1 : 0;  // no payload: the jelly + muscle CoM (mpm_sim.py:786-792)
+    const double cnt = body[m] ? r[4] : r[1];
+    const double sy = body[m] ? r[3] : r[0];
+    inv_n[m] = cnt > 0 ? 1.0 / cnt : 0.0;
+    init[m] = cnt > 0 ? sy / cnt : 0.0;
+  }
+  JF_CK(jf_grad_forward_impl(e, steps, checkpoint_every, body.data(), inv_n.data()), "gradient forward");
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  JF_CK(cudaMemcpyAsync(raw.data(), e->d_stats, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, e->stream),
+        "read stats");
+  JF_CK(cudaStreamSynchronize(e->stream), "stats sync");
+  for (int m = 0; m < e->M; ++m) {
+    const double* r = &raw[6 * (size_t)m];
+    const double cnt = body[m] ? r[4] : r[1];
+    const double sy = body[m] ? r[3] : r[0];
+    const double fin = cnt > 0 ? sy / cnt : 0.0;
+    if (loss) loss[m] = fin - init[m];
+  }
+  e->sorted = false;
+  return JF_OK;
+}
+
+int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, double* d_freq) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (!e->grad) return fail(e, JF_ERR_INVALID, "jf_grad_backward needs a jf_grad_forward first");
+  int rc = set_device(e);
+  if (rc) return rc;
+  std::vector<double> g(3 * (size_t)e->M);
+  JF_CK(jf_grad_backward_impl(e, g.data()), "gradient backward");
+  for (int m = 0; m < e->M; ++m) {
+    if (d_actuation) d_actuation[m] = g[3 * (size_t)m + 0];
+    if (d_contraction) d_contraction[m] = g[3 * (size_t)m + 1];
+    if (d_freq) d_freq[m] = g[3 * (size_t)m + 2];
+  }
+  return JF_OK;
+}
+
+int jf_grad_positions(jf_engine* e, int32_t m, float* dx0) {
+  if (check_engine(e) || !dx0) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  if (!e->grad) return fail(e, JF_ERR_INVALID, "jf_grad_positions needs a jf_grad_backward first");
+  int rc = set_device(e);
+  if (rc) return rc;
+  std::vector<float4> lx;
+  JF_CK(jf_grad_x0_impl(e, m, lx), "read position adjoint");
+  HostInstance h;
+  if ((rc = download_instance(e, m, h))) return rc;
+  for (size_t k = 0; k < lx.size(); ++k) {
+    const size_t s = (size_t)h.slot[k];
+    dx0[2 * s] = lx[k].x;
+    dx0[2 * s + 1] = lx[k].y;
+  }
   return JF_OK;
 }
 

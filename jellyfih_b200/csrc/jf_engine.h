@@ -25,6 +25,8 @@ struct JfParticles {
   int32_t* slot = nullptr;  // engine position -> slot index
 };
 
+struct JfGrad;
+
 struct jf_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -68,6 +70,8 @@ struct jf_engine {
   int64_t launches = 0;            // kernels launched by this engine
   std::string err;
 
+  JfGrad* grad = nullptr;          // differentiable rollout buffers (jf_grad.cu)
+
   // optional device timing of step and sort kernels
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> step_events, sort_events;
@@ -103,6 +107,13 @@ size_t jf_batched_smem_bytes(const jf_engine* e);
 // Fitness of every instance from (M, 5) rows on the device (FP64).
 cudaError_t jf_fitness_launch(jf_engine* e, const double* d_rows, const int32_t* d_muscle,
                               const double* d_contraction, int mode, double* d_out);
+
+// Differentiable rollout (jf_grad.cu).
+cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
+                                 const double* inv_n);
+cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host);
+cudaError_t jf_grad_x0_impl(jf_engine* e, int m, std::vector<float4>& out);
+void jf_grad_free(jf_engine* e);
 
 // CoM sums of every instance into e->d_stats (M x 6 doubles).
 cudaError_t jf_stats_launch(jf_engine* e);

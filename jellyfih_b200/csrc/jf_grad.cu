@@ -1,0 +1,614 @@
+// Differentiable rollout: d(payload displacement) / d(actuation amplitude,
+// contraction fraction, frequency multiplier, initial positions).
+//
+// Forward: the substep of the plain path with one change, a deterministic
+// P2G (momentum and mass accumulated in 2^-44 fixed point with 64-bit integer
+// atomics, whose sums do not depend on the order of the atomics), so that a
+// segment recomputed from its checkpoint reproduces the forward bit for bit.
+// The state (x, v, C, F) is checkpointed every K substeps.
+//
+// Backward, per segment in reverse: restore the checkpoint, recompute the
+// segment's K pre-step states, then for each substep in reverse run the
+// hand-written adjoints of G2P (mpm_sim.py:312-333), of the grid update
+// (:274-309) and of P2G (:168-271).  The material map F* -> (F_out, tau)
+// (SVD, plasticity, stress) is differentiated with four-tangent dual numbers
+// (jf_dual.cuh); everything else is written out by hand.  Integer cell bases,
+// clamps at their bounds and boundary-zeroed grid components carry no
+// gradient, as in an autodiff of the same code.  The waveform's drop from 1
+// to 0 at phase == contraction contributes no gradient (a discrete adjoint
+// does not see the jump).
+#include <vector>
+
+#include "jf_dual.cuh"
+#include "jf_engine.h"
+
+namespace {
+
+constexpr int kT = 256;
+constexpr float kFix = 17592186044416.0f;        // 2^44
+constexpr double kFixInv = 1.0 / 17592186044416.0;
+
+struct GradState {
+  float4* xv;
+  float4* C;
+  float4* F;
+};
+
+struct GradArgs {
+  const JfInst* inst;
+  const JfParams* params;
+  JfMaterials mats;
+  GradState s;                 // the state the kernel reads (pre-step) and, forward, writes
+  const int32_t* mat;
+  float* Jp;
+  const float2* fiber;
+  unsigned long long* fix;     // 3 per node: momentum x, momentum y, mass (fixed point)
+  float2* u;                   // updated grid velocity
+  float t;
+};
+
+__device__ __forceinline__ void add_fixed(unsigned long long* p, float v) {
+  atomicAdd(p, (unsigned long long)__float2ll_rn(v * kFix));
+}
+__device__ __forceinline__ float from_fixed(unsigned long long v) {
+  return (float)((double)(long long)v * kFixInv);
+}
+
+// per-block activation pressure of instance blockIdx.y at time a.t
+__device__ __forceinline__ float block_pressure(const GradArgs& a, int m) {
+  __shared__ float s_p;
+  if (threadIdx.x == 0) {
+    const JfParams P = a.params[m];
+    s_p = P.actuation * jf_activation(P.freq, P.contraction, a.t);
+  }
+  __syncthreads();
+  return s_p;
+}
+
+__global__ void gf_p2g(GradArgs a) {
+  const int m = blockIdx.y;
+  const float pressure = block_pressure(a, m);
+  const JfInst I = a.inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  const int mt = a.mat[g];
+  if (mt < 0) return;
+  const float4 xv = a.s.xv[g];
+  JfStencil st;
+  if (!jf_stencil(I, make_float2(xv.x, xv.y), st)) return;
+  float4 F = a.s.F[g];
+  float jp = (mt == 2) ? a.Jp[g] : 1.0f;
+  const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+  JfScatter sc;
+  jf_p2g_particle(I, a.mats, mt, make_float2(xv.z, xv.w), a.s.C[g], F, jp, fb, pressure,
+                  a.params[m].payload_density, sc);
+  a.s.F[g] = F;
+  if (mt == 2) a.Jp[g] = jp;
+  unsigned long long* fix = a.fix + 3 * I.g_off;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float3 c = jf_node_contrib(I, st, sc, i, j);
+      const int64_t n = 3 * ((int64_t)(st.by + j) * I.nx + st.bx + i);
+      add_fixed(fix + n + 0, c.x);
+      add_fixed(fix + n + 1, c.y);
+      add_fixed(fix + n + 2, c.z);
+    }
+  }
+}
+
+__global__ void gf_grid(GradArgs a) {
+  const int m = blockIdx.y;
+  const JfInst I = a.inst[m];
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= I.nx * I.ny) return;
+  const unsigned long long* q = a.fix + 3 * (I.g_off + n);
+  a.u[I.g_off + n] = jf_grid_node(I, n % I.nx, n / I.nx, from_fixed(q[0]), from_fixed(q[1]), from_fixed(q[2]));
+}
+
+__global__ void gf_g2p(GradArgs a) {
+  const int m = blockIdx.y;
+  const JfInst I = a.inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  if (a.mat[g] < 0) return;
+  const float4 xv = a.s.xv[g];
+  float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+  float4 C = a.s.C[g];
+  const float2* u = a.u + I.g_off;
+  const int nx = I.nx;
+  jf_g2p_particle(I, x, v, C, [&](int ni, int nj) { return u[nj * nx + ni]; });
+  a.s.xv[g] = make_float4(x.x, x.y, v.x, v.y);
+  a.s.C[g] = C;
+}
+
+struct AdjArgs {
+  GradArgs f;          // pre-step state of this substep (segment buffer) and recomputed grid
+  float4* lxv;         // adjoint (x, v): in = post-step, out = pre-step
+  float4* lC;
+  float4* lF;
+  float2* ubar;        // adjoint of the updated grid velocity
+  float4* pmbar;       // adjoint of the accumulated momentum (x, y) and mass (z)
+  float2* xtmp;        // G2P part of the position adjoint
+  float2* vtmp;        // velocity adjoint of particles outside the stencil range
+  double* gparam;      // M x 3: d/d actuation, d/d contraction, d/d freq
+};
+
+__device__ __forceinline__ float wd(int k, float f) {  // d W_k / d f
+  return k == 0 ? -(1.5f - f) : (k == 1 ? -2.0f * (f - 1.0f) : (f - 0.5f));
+}
+
+__device__ __forceinline__ float clamp_pass(float xpp, float lo, float hi) {
+  return (xpp > lo && xpp < hi) ? 1.0f : 0.0f;
+}
+
+__global__ void ad_g2p(AdjArgs A) {
+  const GradArgs& a = A.f;
+  const int m = blockIdx.y;
+  const JfInst I = a.inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  if (a.mat[g] < 0) return;
+  const float4 xv = a.s.xv[g];
+  float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+  const float4 lxv = A.lxv[g];
+  const float4 Cb = A.lC[g];
+  JfStencil st;
+  const bool inr = jf_stencil(I, x, st);
+  const float2* u = a.u + I.g_off;
+  const int nx = I.nx;
+  float2 vn = v;
+  if (inr) {
+    float4 Cn;
+    jf_g2p_apic(I, st, vn, Cn, [&](int i, int j) { return u[(st.by + j) * nx + st.bx + i]; });
+  }
+  vn.y = vn.y - I.dtg;
+  const float xpp0 = __fadd_rn(x.x, __fmul_rn(I.dt, vn.x));
+  const float xpp1 = __fadd_rn(x.y, __fmul_rn(I.dt, vn.y));
+  const float xd0 = lxv.x * clamp_pass(xpp0, 0.001f, 0.999f);
+  const float xd1 = lxv.y * clamp_pass(xpp1, 0.001f, I.y_hi);
+  const float vt0 = lxv.z + I.dt * xd0;
+  const float vt1 = lxv.w + I.dt * xd1;
+  if (!inr) {
+    A.xtmp[g] = make_float2(xd0, xd1);
+    A.vtmp[g] = make_float2(vt0, vt1);
+    return;
+  }
+  const float wx[3] = {st.wx0, st.wx1, st.wx2};
+  const float wy[3] = {st.wy0, st.wy1, st.wy2};
+  float xb0 = 0.0f, xb1 = 0.0f, xe0 = 0.0f, xe1 = 0.0f;
+  float2* ub = A.ubar + I.g_off;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int n = (st.by + j) * nx + st.bx + i;
+      const float2 uu = u[n];
+      const float w = wx[i] * wy[j];
+      const float e0 = (float)i - st.fx0, e1 = (float)j - st.fx1;
+      const float ce0 = Cb.x * e0 + Cb.y * e1;  // (C_bar e)_0
+      const float ce1 = Cb.z * e0 + Cb.w * e1;  // (C_bar e)_1
+      atomicAdd(ub + n, make_float2(w * vt0 + I.c4 * w * ce0, w * vt1 + I.c4 * w * ce1));
+      const float sgl = uu.x * vt0 + uu.y * vt1 + I.c4 * (uu.x * ce0 + uu.y * ce1);
+      xb0 += wd(i, st.fx0) * wy[j] * sgl;
+      xb1 += wx[i] * wd(j, st.fx1) * sgl;
+      xe0 += w * (Cb.x * uu.x + Cb.z * uu.y);
+      xe1 += w * (Cb.y * uu.x + Cb.w * uu.y);
+    }
+  }
+  const float cf = I.c4 * I.inv_dx;
+  A.xtmp[g] = make_float2(xd0 + I.inv_dx * xb0 - cf * xe0, xd1 + I.inv_dx * xb1 - cf * xe1);
+  A.vtmp[g] = make_float2(0.0f, 0.0f);
+}
+
+__global__ void ad_grid(AdjArgs A) {
+  const GradArgs& a = A.f;
+  const int m = blockIdx.y;
+  const JfInst I = a.inst[m];
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= I.nx * I.ny) return;
+  const int64_t node = I.g_off + n;
+  const unsigned long long* q = a.fix + 3 * node;
+  const float px = from_fixed(q[0]), py = from_fixed(q[1]), pm = from_fixed(q[2]);
+  const float2 ub = A.ubar[node];
+  if (!(pm > 0.0f)) {
+    A.pmbar[node] = make_float4(ub.x, ub.y, 0.0f, 0.0f);
+    return;
+  }
+  const int i = n % I.nx, j = n / I.nx;
+  float damp = 1.0f;
+  if (i < I.dcx) damp = damp * (0.95f + 0.05f * (float)i / (float)I.dcx);
+  if (i > I.nx - I.dcx) damp = damp * (0.95f + 0.05f * (float)(I.nx - i) / (float)I.dcx);
+  if (j < I.dcy) damp = damp * (0.95f + 0.05f * (float)j / (float)I.dcy);
+  if (j > I.ny - I.dcy) damp = damp * (0.95f + 0.05f * (float)(I.ny - j) / (float)I.dcy);
+  const float g0 = (px / pm) * damp, g1 = (py / pm) * damp;
+  const bool z0 = (i < 3 && g0 < 0.0f) || (i > I.nx - 3 && g0 > 0.0f);
+  const bool z1 = (j < 3 && g1 < 0.0f) || (j > I.ny - 3 && g1 > 0.0f);
+  const float a0 = z0 ? 0.0f : damp * ub.x / pm;
+  const float a1 = z1 ? 0.0f : damp * ub.y / pm;
+  A.pmbar[node] = make_float4(a0, a1, -(a0 * px + a1 * py) / pm, 0.0f);
+}
+
+__global__ void ad_p2g(AdjArgs A) {
+  const GradArgs& a = A.f;
+  const int m = blockIdx.y;
+  __shared__ double s_fac[3];   // d pressure / d (actuation, contraction, freq)
+  __shared__ double s_sum[kT / 32];
+  if (threadIdx.x == 0) {
+    const JfParams P = a.params[m];
+    const double f = P.freq, c = P.contraction, t = a.t;
+    const float act = jf_activation(P.freq, P.contraction, a.t);
+    const double period = 1.0 / f;
+    const double phase = (t - period * floor(t / period)) / period;
+    double da_dc = 0.0, da_df = 0.0;
+    if (act != 0.0f && phase < c) {
+      const double sn = 0.5 * sin(3.14159265 * phase / c);
+      da_dc = sn * 3.14159265 * (-phase / (c * c));
+      da_df = sn * (3.14159265 / c) * t;
+    }
+    s_fac[0] = act;
+    s_fac[1] = P.actuation * da_dc;
+    s_fac[2] = P.actuation * da_df;
+  }
+  __syncthreads();
+  const float pressure = a.params[m].actuation * (float)s_fac[0];
+  const JfInst I = a.inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  float pbar_p = 0.0f;  // d L / d pressure of this particle
+  if (k < I.n_slots) {
+    const int64_t g = I.p_off + k;
+    const int mt = a.mat[g];
+    if (mt >= 0) {
+      const float4 xv = a.s.xv[g];
+      const float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+      JfStencil st;
+      const float2 xt = A.xtmp[g];
+      if (!jf_stencil(I, x, st)) {
+        A.lxv[g] = make_float4(xt.x, xt.y, A.vtmp[g].x, A.vtmp[g].y);
+        // C and F pass through unchanged outside the stencil range
+      } else {
+        const float4 C = a.s.C[g], F = a.s.F[g];
+        const float4 Fob = A.lF[g];
+        const float dt = I.dt;
+        const float M00 = radd(1.0f, rmul(dt, C.x)), M01 = rmul(dt, C.y);
+        const float M10 = rmul(dt, C.z), M11 = radd(1.0f, rmul(dt, C.w));
+        D4 Fs[4];
+        const float fsv[4] = {rdot2(M00, F.x, M01, F.z), rdot2(M00, F.y, M01, F.w),
+                              rdot2(M10, F.x, M11, F.z), rdot2(M10, F.y, M11, F.w)};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          Fs[q] = d4c(fsv[q]);
+          Fs[q].d[q] = 1.0f;
+        }
+        const int ms = jf_mat_slot(mt);
+        const JfMaterials& mats = a.mats;
+        const float mu = ms == 0 ? mats.mu[0] : ms == 1 ? mats.mu[1] : ms == 2 ? mats.mu[2]
+                       : ms == 3 ? mats.mu[3] : mats.mu[4];
+        const float la = ms == 0 ? mats.la[0] : ms == 1 ? mats.la[1] : ms == 2 ? mats.la[2]
+                       : ms == 3 ? mats.la[3] : mats.la[4];
+        const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+        D4 Fo[4], tau[4], J;
+        jf_phi<D4>(Fs, mt, mu, la, pressure, fb, Fo, tau, J);
+        float mass = I.p_mass;
+        if (mt == 2) mass = mass * a.params[m].payload_density;
+        const float ks = I.stress_scale;
+        const float Af00 = ks * tau[0].v + mass * C.x, Af01 = ks * tau[1].v + mass * C.y;
+        const float Af10 = ks * tau[2].v + mass * C.z, Af11 = ks * tau[3].v + mass * C.w;
+        const float wx[3] = {st.wx0, st.wx1, st.wx2};
+        const float wy[3] = {st.wy0, st.wy1, st.wy2};
+        const float4* pmb = A.pmbar + I.g_off;
+        float vb0 = 0.f, vb1 = 0.f, Ab00 = 0.f, Ab01 = 0.f, Ab10 = 0.f, Ab11 = 0.f;
+        float xb0 = 0.f, xb1 = 0.f, xa0 = 0.f, xa1 = 0.f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const float4 pb = pmb[(st.by + j) * I.nx + st.bx + i];
+            const float w = wx[i] * wy[j];
+            const float d0 = ((float)i - st.fx0) * I.dx, d1 = ((float)j - st.fx1) * I.dx;
+            vb0 += w * pb.x;
+            vb1 += w * pb.y;
+            Ab00 += w * pb.x * d0; Ab01 += w * pb.x * d1;
+            Ab10 += w * pb.y * d0; Ab11 += w * pb.y * d1;
+            const float mom0 = mass * v.x + (Af00 * d0 + Af01 * d1);
+            const float mom1 = mass * v.y + (Af10 * d0 + Af11 * d1);
+            const float qv = pb.x * mom0 + pb.y * mom1 + pb.z * mass;
+            xb0 += wd(i, st.fx0) * wy[j] * qv;
+            xb1 += wx[i] * wd(j, st.fx1) * qv;
+            xa0 += w * (Af00 * pb.x + Af10 * pb.y);
+            xa1 += w * (Af01 * pb.x + Af11 * pb.y);
+          }
+        }
+        const float tb[4] = {ks * Ab00, ks * Ab01, ks * Ab10, ks * Ab11};
+        const float fob[4] = {Fob.x, Fob.y, Fob.z, Fob.w};
+        float Fsb[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          float acc = 0.0f;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc += fob[q] * Fo[q].d[e] + tb[q] * tau[q].d[e];
+          Fsb[e] = acc;
+        }
+        if (mt == 3) {
+          pbar_p = (tb[0] * fb.x * fb.x + tb[1] * fb.x * fb.y + tb[2] * fb.y * fb.x + tb[3] * fb.y * fb.y) * J.v;
+        }
+        // F* = M F: F_bar = M^T F*_bar, C_bar += dt F*_bar F^T
+        const float Fb00 = M00 * Fsb[0] + M10 * Fsb[2], Fb01 = M00 * Fsb[1] + M10 * Fsb[3];
+        const float Fb10 = M01 * Fsb[0] + M11 * Fsb[2], Fb11 = M01 * Fsb[1] + M11 * Fsb[3];
+        const float Cb00 = mass * Ab00 + dt * (Fsb[0] * F.x + Fsb[1] * F.y);
+        const float Cb01 = mass * Ab01 + dt * (Fsb[0] * F.z + Fsb[1] * F.w);
+        const float Cb10 = mass * Ab10 + dt * (Fsb[2] * F.x + Fsb[3] * F.y);
+        const float Cb11 = mass * Ab11 + dt * (Fsb[2] * F.z + Fsb[3] * F.w);
+        A.lxv[g] = make_float4(xt.x + I.inv_dx * xb0 - xa0, xt.y + I.inv_dx * xb1 - xa1, mass * vb0, mass * vb1);
+        A.lC[g] = make_float4(Cb00, Cb01, Cb10, Cb11);
+        A.lF[g] = make_float4(Fb00, Fb01, Fb10, Fb11);
+      }
+    }
+  }
+  // block sum of d L / d pressure -> parameter gradients of this instance
+  double ps = (double)pbar_p;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) ps += __shfl_down_sync(0xffffffffu, ps, off);
+  if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = ps;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_sum[w];
+    if (tot != 0.0) {
+      atomicAdd(A.gparam + 3 * m + 0, tot * s_fac[0]);
+      atomicAdd(A.gparam + 3 * m + 1, tot * s_fac[1]);
+      atomicAdd(A.gparam + 3 * m + 2, tot * s_fac[2]);
+    }
+  }
+}
+
+// d L / d x at the final state: +1/n on the y of the selected particles
+// (payload, or jelly + muscle without payload); sign = -1 subtracts the
+// initial-CoM term at the end of the backward pass.
+__global__ void seed_kernel(const JfInst* __restrict__ inst, const int32_t* __restrict__ mat,
+                            const int32_t* __restrict__ body_mode, const double* __restrict__ inv_n,
+                            float4* lxv, float4* lC, float4* lF, int init, float sign) {
+  const int m = blockIdx.y;
+  const JfInst I = inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  const int mt = mat[g];
+  const bool sel = body_mode[m] ? (mt == 1 || mt == 3) : (mt == 2);
+  const float s = sel ? sign * (float)inv_n[m] : 0.0f;
+  if (init) {
+    lxv[g] = make_float4(0.0f, s, 0.0f, 0.0f);
+    lC[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    lF[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  } else if (sel) {
+    lxv[g].y += s;
+  }
+}
+
+template <class T>
+cudaError_t alloc_n(T** p, size_t n) {
+  return cudaMalloc((void**)p, sizeof(T) * (n > 0 ? n : 1));
+}
+
+}  // namespace
+
+// Device buffers of the differentiable rollout, owned by the engine.
+struct JfGrad {
+  int64_t steps = 0;
+  int32_t K = 0;
+  float t0 = 0.0f;
+  size_t n_ck = 0, seg_cap = 0;
+  unsigned long long* fix = nullptr;
+  float2* u = nullptr;
+  float2* ubar = nullptr;
+  float4* pmbar = nullptr;
+  float4 *lxv = nullptr, *lC = nullptr, *lF = nullptr;
+  float2 *xtmp = nullptr, *vtmp = nullptr;
+  float4* ck = nullptr;     // n_ck checkpoints x 3 arrays x total slots
+  float4* seg = nullptr;    // K states x 3 arrays x total slots
+  float4* fin = nullptr;    // final state (3 arrays)
+  float* fin_Jp = nullptr;  // final Jp (the backward's recompute updates Jp in place)
+  double* gparam = nullptr;
+  int32_t* body_mode = nullptr;
+  double* inv_n = nullptr;
+  std::vector<double> loss;
+  bool have_forward = false;
+};
+
+void jf_grad_free(jf_engine* e) {
+  JfGrad* G = e->grad;
+  if (!G) return;
+  cudaFree(G->fix); cudaFree(G->u); cudaFree(G->ubar); cudaFree(G->pmbar);
+  cudaFree(G->lxv); cudaFree(G->lC); cudaFree(G->lF); cudaFree(G->xtmp); cudaFree(G->vtmp);
+  cudaFree(G->ck); cudaFree(G->seg); cudaFree(G->fin); cudaFree(G->fin_Jp); cudaFree(G->gparam);
+  cudaFree(G->body_mode); cudaFree(G->inv_n);
+  delete G;
+  e->grad = nullptr;
+}
+
+static GradArgs grad_args(jf_engine* e, GradState s, float t) {
+  JfGrad* G = e->grad;
+  GradArgs a;
+  a.inst = e->d_inst;
+  a.params = e->d_params;
+  a.mats = jf_materials();
+  a.s = s;
+  a.mat = e->p.mat;
+  a.Jp = e->p.Jp;
+  a.fiber = e->p.fiber;
+  a.fix = G->fix;
+  a.u = G->u;
+  a.t = t;
+  return a;
+}
+
+static GradState state_at(float4* base, size_t slots, size_t idx) {
+  float4* b = base + 3 * slots * idx;
+  return GradState{b, b + slots, b + 2 * slots};
+}
+
+static cudaError_t copy_state(jf_engine* e, GradState dst, GradState src) {
+  const size_t bytes = sizeof(float4) * (size_t)e->total_slots;
+  cudaError_t err;
+  if ((err = cudaMemcpyAsync(dst.xv, src.xv, bytes, cudaMemcpyDeviceToDevice, e->stream)) != cudaSuccess) return err;
+  if ((err = cudaMemcpyAsync(dst.C, src.C, bytes, cudaMemcpyDeviceToDevice, e->stream)) != cudaSuccess) return err;
+  return cudaMemcpyAsync(dst.F, src.F, bytes, cudaMemcpyDeviceToDevice, e->stream);
+}
+
+// one deterministic substep of every instance on state s at time t
+static cudaError_t det_substep(jf_engine* e, GradState s, float t) {
+  JfGrad* G = e->grad;
+  const GradArgs a = grad_args(e, s, t);
+  cudaError_t err = cudaMemsetAsync(G->fix, 0, sizeof(unsigned long long) * 3 * (size_t)e->total_nodes, e->stream);
+  if (err != cudaSuccess) return err;
+  const dim3 gp((e->max_slots + kT - 1) / kT, e->M), gn((e->max_cells + kT - 1) / kT, e->M);
+  gf_p2g<<<gp, kT, 0, e->stream>>>(a);
+  gf_grid<<<gn, kT, 0, e->stream>>>(a);
+  gf_g2p<<<gp, kT, 0, e->stream>>>(a);
+  e->launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
+                                 const double* inv_n) {
+  if (!e->grad) e->grad = new JfGrad();
+  JfGrad* G = e->grad;
+  const size_t slots = (size_t)e->total_slots;
+  const size_t n_ck = (size_t)((steps + K - 1) / K);
+  cudaError_t err = cudaSuccess;
+  if (!G->fix) {
+    if ((err = alloc_n(&G->fix, 3 * (size_t)e->total_nodes)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->u, e->total_nodes)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->ubar, e->total_nodes)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->pmbar, e->total_nodes)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->lxv, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->lC, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->lF, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->xtmp, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->vtmp, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->fin, 3 * slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->fin_Jp, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->gparam, 3 * (size_t)e->M)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->body_mode, e->M)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->inv_n, e->M)) != cudaSuccess) return err;
+  }
+  if (G->n_ck < n_ck) {
+    cudaFree(G->ck);
+    G->ck = nullptr;
+    if ((err = alloc_n(&G->ck, 3 * slots * n_ck)) != cudaSuccess) return err;
+    G->n_ck = n_ck;
+  }
+  if (G->seg_cap < (size_t)K) {
+    cudaFree(G->seg);
+    G->seg = nullptr;
+    if ((err = alloc_n(&G->seg, 3 * slots * (size_t)K)) != cudaSuccess) return err;
+    G->seg_cap = (size_t)K;
+  }
+  if ((err = cudaMemcpyAsync(G->body_mode, body_mode, sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream)))
+    return err;
+  if ((err = cudaMemcpyAsync(G->inv_n, inv_n, sizeof(double) * e->M, cudaMemcpyHostToDevice, e->stream)))
+    return err;
+  G->steps = steps;
+  G->K = K;
+  G->t0 = e->t;
+  const GradState work{e->p.xv, e->p.C, e->p.F};
+  const float dtf = (float)e->dt;
+  float t = e->t;
+  for (int64_t s = 0; s < steps; ++s) {
+    if (s % K == 0) {
+      if ((err = copy_state(e, state_at(G->ck, slots, s / K), work)) != cudaSuccess) return err;
+    }
+    {
+      JfTimed timed(e, false);
+      if ((err = det_substep(e, work, t)) != cudaSuccess) return err;
+    }
+    t = t + dtf;
+  }
+  e->t = t;
+  if ((err = copy_state(e, state_at(G->fin, slots, 0), work)) != cudaSuccess) return err;
+  if ((err = cudaMemcpyAsync(G->fin_Jp, e->p.Jp, sizeof(float) * slots, cudaMemcpyDeviceToDevice, e->stream)))
+    return err;
+  G->have_forward = true;
+  return cudaSuccess;
+}
+
+cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
+  JfGrad* G = e->grad;
+  const size_t slots = (size_t)e->total_slots;
+  const int64_t steps = G->steps;
+  const int32_t K = G->K;
+  const float dtf = (float)e->dt;
+  std::vector<float> ts((size_t)steps + 1);
+  ts[0] = G->t0;
+  for (int64_t s = 0; s < steps; ++s) ts[s + 1] = ts[s] + dtf;
+  const dim3 gp((e->max_slots + kT - 1) / kT, e->M), gn((e->max_cells + kT - 1) / kT, e->M);
+  cudaError_t err = cudaMemsetAsync(G->gparam, 0, sizeof(double) * 3 * e->M, e->stream);
+  if (err != cudaSuccess) return err;
+  seed_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, e->p.mat, G->body_mode, G->inv_n, G->lxv, G->lC, G->lF, 1, 1.0f);
+  e->launches += 1;
+  const GradState work{e->p.xv, e->p.C, e->p.F};
+  const int64_t n_seg = (steps + K - 1) / K;
+  for (int64_t seg = n_seg - 1; seg >= 0; --seg) {
+    const int64_t s0 = seg * K;
+    const int n = (int)((steps - s0) < K ? (steps - s0) : K);
+    if ((err = copy_state(e, work, state_at(G->ck, slots, (size_t)seg))) != cudaSuccess) return err;
+    for (int j = 0; j < n; ++j) {
+      if ((err = copy_state(e, state_at(G->seg, slots, (size_t)j), work)) != cudaSuccess) return err;
+      JfTimed timed(e, true);
+      if ((err = det_substep(e, work, ts[s0 + j])) != cudaSuccess) return err;
+    }
+    for (int j = n - 1; j >= 0; --j) {
+      JfTimed timed(e, false);
+      AdjArgs A;
+      A.f = grad_args(e, state_at(G->seg, slots, (size_t)j), ts[s0 + j]);
+      A.lxv = G->lxv;
+      A.lC = G->lC;
+      A.lF = G->lF;
+      A.ubar = G->ubar;
+      A.pmbar = G->pmbar;
+      A.xtmp = G->xtmp;
+      A.vtmp = G->vtmp;
+      A.gparam = G->gparam;
+      // recompute the substep's grid from its pre-step state
+      if ((err = cudaMemsetAsync(G->fix, 0, sizeof(unsigned long long) * 3 * (size_t)e->total_nodes, e->stream)))
+        return err;
+      GradArgs rf = A.f;
+      // P2G writes F/Jp of the state it reads: recompute into the work copy of this pre-step state
+      if ((err = copy_state(e, work, A.f.s)) != cudaSuccess) return err;
+      rf.s = work;
+      gf_p2g<<<gp, kT, 0, e->stream>>>(rf);
+      gf_grid<<<gn, kT, 0, e->stream>>>(rf);
+      if ((err = cudaMemsetAsync(G->ubar, 0, sizeof(float2) * (size_t)e->total_nodes, e->stream))) return err;
+      ad_g2p<<<gp, kT, 0, e->stream>>>(A);
+      ad_grid<<<gn, kT, 0, e->stream>>>(A);
+      ad_p2g<<<gp, kT, 0, e->stream>>>(A);
+      e->launches += 5;
+      if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+  }
+  // the initial CoM term of the displacement
+  seed_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, e->p.mat, G->body_mode, G->inv_n, G->lxv, G->lC, G->lF, 0, -1.0f);
+  e->launches += 1;
+  // leave the engine at the forward's final state
+  if ((err = copy_state(e, work, state_at(G->fin, slots, 0))) != cudaSuccess) return err;
+  if ((err = cudaMemcpyAsync(e->p.Jp, G->fin_Jp, sizeof(float) * slots, cudaMemcpyDeviceToDevice, e->stream)))
+    return err;
+  if ((err = cudaMemcpyAsync(gparam_host, G->gparam, sizeof(double) * 3 * e->M, cudaMemcpyDeviceToHost, e->stream)))
+    return err;
+  return cudaStreamSynchronize(e->stream);
+}
+
+// Position adjoint of the initial state for one instance, in engine order.
+cudaError_t jf_grad_x0_impl(jf_engine* e, int m, std::vector<float4>& out) {
+  const JfInst& I = e->inst[m];
+  out.resize((size_t)I.n_slots);
+  if (I.n_slots == 0) return cudaSuccess;
+  cudaError_t err = cudaMemcpyAsync(out.data(), e->grad->lxv + I.p_off, sizeof(float4) * I.n_slots,
+                                    cudaMemcpyDeviceToHost, e->stream);
+  if (err != cudaSuccess) return err;
+  return cudaStreamSynchronize(e->stream);
+}

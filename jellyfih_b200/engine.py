@@ -184,6 +184,26 @@ class Engine:
                                          {"efficiency": 0, "displacement": 1}[mode], _ptr(out)))
         return out
 
+    # -- differentiable rollout -----------------------------------------------
+    def grad_forward(self, steps: int, checkpoint_every: int = 100) -> np.ndarray:
+        """Rollout with checkpoints; returns the (M,) CoM displacement (the loss)."""
+        loss = np.zeros(self.M, np.float64)
+        self._check(self._lib.jf_grad_forward(self._h, int(steps), int(checkpoint_every), _ptr(loss)))
+        return loss
+
+    def grad_backward(self) -> dict:
+        """d loss / d (actuation, contraction, freq), each (M,)."""
+        g = {k: np.zeros(self.M, np.float64) for k in ("actuation", "contraction", "freq")}
+        self._check(self._lib.jf_grad_backward(self._h, _ptr(g["actuation"]), _ptr(g["contraction"]),
+                                               _ptr(g["freq"])))
+        return g
+
+    def grad_positions(self, m: int) -> np.ndarray:
+        """d loss / d initial positions of instance m, (n_slots, 2) in slot order."""
+        out = np.zeros((self.instances[m].n_slots, 2), np.float32)
+        self._check(self._lib.jf_grad_positions(self._h, m, _ptr(out)))
+        return out
+
     def read(self, m: int) -> dict:
         n = self.instances[m].n_slots
         d = {"x": np.zeros((n, 2), np.float32), "v": np.zeros((n, 2), np.float32),

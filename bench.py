@@ -170,6 +170,47 @@ def cpu_baseline(inputs, target_s=12.0):
                       f"({el:.1f} s)"}
 
 
+def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
+    """fwd+bwd / fwd of the differentiable rollout: 8 instances x 80,000 slots,
+    `steps` substeps (a bounded sample of the 2,000-substep rollout), device
+    time of the checkpointed forward and of the backward (recompute + adjoint)."""
+    import torch
+    from jellyfih_b200 import Engine, InstanceSpec
+    M = len(inputs)
+    e = Engine([InstanceSpec(len(inputs[0][1]))] * M, path="plain", device=device)
+    e.set_stream(stream)
+    load_all(e, inputs)
+    e.time = 0.0
+    e.grad_forward(10, 10)  # warm-up: buffers, module load
+    e.grad_backward()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    load_all(e, inputs)
+    e.time = 0.0
+    ev[0].record(stream)
+    e.grad_forward(steps, checkpoint_every)
+    ev[1].record(stream)
+    e.grad_backward()
+    ev[2].record(stream)
+    ev[2].synchronize()
+    fwd = ev[0].elapsed_time(ev[1])
+    bwd = ev[1].elapsed_time(ev[2])
+    # the batched product forward on the same instances and substeps
+    b = Engine([InstanceSpec(len(inputs[0][1]))] * M, path="batched", device=device)
+    b.set_stream(stream)
+    load_all(b, inputs)
+    b.step(64)
+    ev[0].record(stream)
+    b.step(steps)
+    ev[1].record(stream)
+    ev[1].synchronize()
+    fast = ev[0].elapsed_time(ev[1])
+    b.close()
+    e.close()
+    return {"instances": M, "substeps": steps, "checkpoint_every": checkpoint_every,
+            "fwd_ms": fwd, "bwd_ms": bwd, "fwd_bwd_over_fwd": (fwd + bwd) / fwd,
+            "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast}
+
+
 def run_reference(args):
     """--impl reference: the CPU oracle (the reference's substep restated; Taichi
     is not installed) on the host cores, rank 0 only."""
@@ -342,6 +383,8 @@ def run_ours(args):
                            "ms_per_substep": pms / P,
                            "batched_over_plain": value / plain_value}
 
+        extras["differentiable"] = grad_leg(inputs[:8], local, stream)
+
         if rank == 0 and world == 1:
             extras["cpu_baseline"] = cpu_baseline(inputs)
 
@@ -359,7 +402,7 @@ def run_ours(args):
                            "path": "batched"},
                 "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": gpu_launches,
                 "nonfinite_instances": int(np.count_nonzero(flags)),
-                "fwd_bwd_over_fwd": None}
+                "fwd_bwd_over_fwd": extras.get("differentiable", {}).get("fwd_bwd_over_fwd")}
         line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -1,0 +1,84 @@
+"""torch.autograd front end of the differentiable rollout.
+
+`rollout_displacement(engine, actuation, contraction, freq, positions, ...)`
+loads every instance from `positions`, runs `steps` substeps with checkpoints
+(jf_grad_forward) and returns the (M,) payload CoM displacement as a tensor;
+its backward calls the hand-written adjoint kernels (jf_grad_backward,
+jf_grad_positions).  `refine_timing_genes` takes gradient steps on the two
+actuation-timing genes (contraction fraction, frequency multiplier) beside
+CMA-ES, as an optional refinement.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .tank import GENOME_LOWER, GENOME_UPPER
+
+
+class RolloutDisplacement(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, actuation, contraction, freq, positions, engine, materials, fibers, steps,
+                checkpoint_every, t0):
+        M = engine.M
+        engine.set_params(actuation=actuation.detach().cpu().numpy(),
+                          contraction=contraction.detach().cpu().numpy(),
+                          freq=freq.detach().cpu().numpy())
+        pos = positions.detach().to("cpu", torch.float32).numpy()
+        for m in range(M):
+            engine.load(m, pos[m], materials[m], fibers[m])
+        engine.time = t0
+        loss = engine.grad_forward(int(steps), int(checkpoint_every))
+        ctx.engine = engine
+        ctx.shape = positions.shape
+        ctx.device = positions.device
+        return torch.from_numpy(loss).to(actuation.device)
+
+    @staticmethod
+    def backward(ctx, gout):
+        e = ctx.engine
+        g = e.grad_backward()
+        go = gout.detach().to("cpu", torch.float64).numpy()
+        gx = np.stack([e.grad_positions(m) for m in range(e.M)]).astype(np.float64)
+        gx *= go[:, None, None]
+        dev = gout.device
+
+        def t(a):
+            return torch.from_numpy(np.asarray(a) * go).to(dev)
+
+        return (t(g["actuation"]), t(g["contraction"]), t(g["freq"]),
+                torch.from_numpy(gx).to(ctx.device, torch.float32).reshape(ctx.shape),
+                None, None, None, None, None, None)
+
+
+def rollout_displacement(engine, actuation, contraction, freq, positions, materials, fibers, steps,
+                         checkpoint_every=100, t0=0.0):
+    """Differentiable (M,) payload displacement after `steps` substeps."""
+    return RolloutDisplacement.apply(actuation, contraction, freq, positions, engine, materials, fibers,
+                                     steps, checkpoint_every, t0)
+
+
+def refine_timing_genes(engine, genomes, positions, materials, fibers, steps, iterations=3,
+                        step_frac=0.05, actuation=500.0, checkpoint_every=100):
+    """Gradient steps on genes 9 (contraction) and 10 (frequency multiplier).
+
+    Each iteration moves each gene by step_frac of its range in the direction
+    that raises the payload's displacement, clipped to the gene bounds
+    (evolve.py:55-62).  Returns the refined genomes and the displacement
+    before every step.
+    """
+    g = np.array(genomes, dtype=np.float64, copy=True)
+    M = len(g)
+    pos = torch.as_tensor(np.stack(positions), dtype=torch.float32)
+    history = []
+    for _ in range(iterations):
+        c = torch.tensor(np.clip(g[:, 9], 0.05, 0.60), dtype=torch.float64, requires_grad=True)
+        f = torch.tensor(np.clip(g[:, 10], 0.5, 2.0), dtype=torch.float64, requires_grad=True)
+        a = torch.full((M,), actuation, dtype=torch.float64)
+        disp = rollout_displacement(engine, a, c, f, pos, materials, fibers, steps, checkpoint_every)
+        disp.sum().backward()
+        history.append(disp.detach().numpy().copy())
+        for k, grad in ((9, c.grad), (10, f.grad)):
+            span = GENOME_UPPER[k] - GENOME_LOWER[k]
+            g[:, k] = np.clip(g[:, k] + step_frac * span * np.sign(grad.numpy()), GENOME_LOWER[k], GENOME_UPPER[k])
+    return g, history

@@ -1,9 +1,14 @@
 """The CUDA adjoint (jf_grad_*) against the float64 autograd reference.
 
 The reference (oracle/torch_mpm.py) is itself checked against FP64 finite
-differences in test_grad_reference.py.  The CUDA path runs in FP32, so its
-gradients carry FP32 rounding of a stiff system; the tolerances below are
-stated against that.
+differences in test_grad_reference.py.  The CUDA path runs in FP32.  Measured
+on a 32^2 tank over 40 substeps: parameter gradients within 1.4e-6 relative,
+position gradients with a median error of 3e-9 and a maximum of 1.2e-2 of
+their max-norm; over 200 substeps 8.7e-4 relative for the parameters.  The
+loss itself (a 5e-6 displacement, ~170 FP32 ulps of a 0.4 position) differs
+from FP64 by 3e-3 from position rounding alone.  Re-running the adjoint
+accumulates its scatter with float atomics, so two runs agree to ~1e-7, not
+bitwise; the forward (fixed-point P2G) is bitwise reproducible.
 """
 import numpy as np
 import pytest
@@ -54,14 +59,14 @@ def test_adjoint_matches_float64_autograd():
     pos, mat, fib, prm = grad_cases.small_tank()
     loss, g, gx, final, after = _cuda_grads(pos, mat, fib, prm, K=15)
     rloss, rg, rgx = _torch_grads(pos, mat, fib, prm)
-    assert abs(loss - rloss) <= 2e-3 * abs(rloss), (loss, rloss)
+    assert abs(loss - rloss) <= 1e-2 * abs(rloss), (loss, rloss)
     for k in ("actuation", "contraction", "freq"):
-        assert abs(g[k] - rg[k]) <= 2e-2 * abs(rg[k]), (k, g[k], rg[k])
+        assert abs(g[k] - rg[k]) <= 2e-5 * abs(rg[k]), (k, g[k], rg[k])
     live = mat >= 0
     scale = np.abs(rgx[live]).max()
     err = np.abs(gx[live] - rgx[live])
     assert err.max() <= 5e-2 * scale, (err.max(), scale)
-    assert np.median(err) <= 1e-3 * scale
+    assert np.median(err) <= 1e-6 * scale
     # the engine is left at the rollout's final state
     for key in ("x", "v", "C", "F"):
         assert np.array_equal(after[key], final[key]), key
@@ -74,8 +79,8 @@ def test_checkpoint_interval_does_not_change_gradients():
     b = _cuda_grads(pos, mat, fib, prm, K=7)
     assert a[0] == b[0]
     for k in ("actuation", "contraction", "freq"):
-        assert a[1][k] == b[1][k], k
-    assert np.array_equal(a[2], b[2])
+        assert abs(a[1][k] - b[1][k]) <= 1e-5 * abs(a[1][k]), k
+    assert np.abs(a[2] - b[2]).max() <= 1e-5 * np.abs(a[2]).max()
 
 
 def test_batched_engine_gradients_equal_plain():
@@ -84,5 +89,35 @@ def test_batched_engine_gradients_equal_plain():
     b = _cuda_grads(pos, mat, fib, prm, K=10, path="batched")
     assert a[0] == b[0]
     for k in ("actuation", "contraction", "freq"):
-        assert a[1][k] == b[1][k], k
-    assert np.array_equal(a[2], b[2])
+        assert abs(a[1][k] - b[1][k]) <= 1e-5 * abs(a[1][k]), k
+    assert np.abs(a[2] - b[2]).max() <= 1e-5 * np.abs(a[2]).max()
+
+
+def test_autograd_function_and_refinement():
+    from jellyfih_b200 import Engine, InstanceSpec, tank
+    from jellyfih_b200.autograd import refine_timing_genes, rollout_displacement
+    pos, mat, fib, prm = grad_cases.small_tank(seed=6)
+    e = Engine([InstanceSpec(len(mat), 32, 32, 1.0)] * 2, path="plain")
+    act = torch.tensor([prm["actuation"], 700.0], dtype=torch.float64, requires_grad=True)
+    con = torch.tensor([prm["contraction"], 0.4], dtype=torch.float64, requires_grad=True)
+    frq = torch.tensor([prm["freq"], 0.9], dtype=torch.float64, requires_grad=True)
+    x = torch.tensor(np.stack([pos, pos]), requires_grad=True)
+    d = rollout_displacement(e, act, con, frq, x, [mat, mat], [fib, fib], STEPS, 15, T0)
+    (2.0 * d[0] - d[1]).backward()
+    # the same gradients straight from the engine, weighted like the loss above
+    e.set_params(actuation=act.detach().numpy(), contraction=con.detach().numpy(), freq=frq.detach().numpy())
+    for m in range(2):
+        e.load(m, pos, mat, fib)
+    e.time = T0
+    e.grad_forward(STEPS, 15)
+    g = e.grad_backward()
+    for name, t in (("actuation", act), ("contraction", con), ("freq", frq)):
+        np.testing.assert_allclose(t.grad.numpy(), [2 * g[name][0], -g[name][1]], rtol=1e-5)
+    gx0 = e.grad_positions(0)
+    np.testing.assert_allclose(x.grad[0].numpy(), 2 * gx0, rtol=1e-4, atol=1e-5 * np.abs(gx0).max())
+    genomes = [np.r_[tank.AURELIA_GENOME, 0.3, 1.0]] * 2
+    refined, hist = refine_timing_genes(e, genomes, [pos, pos], [mat, mat], [fib, fib], STEPS,
+                                        iterations=2, checkpoint_every=20)
+    assert len(hist) == 2 and np.all(np.isfinite(hist))
+    assert np.all(refined[:, 9] != 0.3) and np.all(refined[:, 10] != 1.0)
+    e.close()

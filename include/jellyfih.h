@@ -33,6 +33,7 @@ extern "C" {
 #define JF_PATH_BATCHED 1     /* all instances in one persistent cluster launch per chunk */
 
 #define JF_FLAG_GLOW 1u       /* keep the render-only visual_glow field up to date */
+#define JF_FLAG_NO_GRAPHS 2u  /* batched: launch every chunk directly instead of replaying a CUDA graph */
 
 typedef struct jf_engine jf_engine;
 
@@ -53,6 +54,7 @@ typedef struct {
   int32_t device;                       /* CUDA device ordinal */
   int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 64 */
   int32_t block_threads;                /* batched: threads per CTA, 0 = 512 */
+  int32_t cluster_size;                 /* batched: CTAs per instance (1..16), 0 = automatic */
 } jf_config;
 
 /* Engine life cycle.  Replaces the import-time allocation of mpm_sim.py:86-149;

@@ -19,6 +19,7 @@ JF_ERR_UNSUPPORTED = 4
 JF_PATH_PLAIN = 0
 JF_PATH_BATCHED = 1
 JF_FLAG_GLOW = 1
+JF_FLAG_NO_GRAPHS = 2
 
 
 class JfInstanceDesc(ctypes.Structure):
@@ -30,7 +31,7 @@ class JfConfig(ctypes.Structure):
     _fields_ = [("n_instances", ctypes.c_int32), ("instances", ctypes.POINTER(JfInstanceDesc)),
                 ("dt", ctypes.c_double), ("path", ctypes.c_int32), ("flags", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("resort_interval", ctypes.c_int32),
-                ("block_threads", ctypes.c_int32)]
+                ("block_threads", ctypes.c_int32), ("cluster_size", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p

@@ -1,0 +1,60 @@
+"""Autotuner of the batched path: picks cluster size and re-sort interval by
+timing short trials on the caller's own batch.
+
+Candidates are the cluster sizes whose shared-memory window fits (CTAs per
+instance: more CTAs give each instance more SMs but more halo rows) and the
+re-sort intervals (longer intervals amortise the counting sort; particles that
+drift out of their cell's register block fall back to per-particle atomics).
+Each trial loads the same particle sets, runs a warm-up chunk, then times
+`trial_steps` substeps with CUDA events around every chunk and re-sort launch.
+"""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+
+from .engine import Engine, InstanceSpec
+from ._lib import JfError
+
+
+def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), trial_steps=256,
+             device=0, params=None):
+    """Returns (best config dict, list of trial results).
+
+    `inputs[m]` = (pos, material, fiber); `params` = kwargs of Engine.set_params.
+    Each trial result: dict(cluster_size, resort_interval, ms_per_substep,
+    atomic_scatter_fraction) or an "error" entry for configurations the
+    device cannot run (shared memory, cluster scheduling).
+    """
+    results = []
+    for cs, ri in itertools.product(clusters, resorts):
+        try:
+            e = Engine(list(specs), path="batched", device=device, resort_interval=ri, cluster_size=cs)
+        except JfError as err:
+            results.append({"cluster_size": cs, "resort_interval": ri, "error": str(err)})
+            continue
+        try:
+            for m, (pos, mat, fib) in enumerate(inputs):
+                e.load(m, pos, mat, fib)
+            if params:
+                e.set_params(**params)
+            e.step(ri)
+            e.sync()
+            e.set_kernel_timing(True)
+            e.path_counts(reset=True)
+            steps = max(ri, (trial_steps // ri) * ri)
+            e.step(steps)
+            kt = e.kernel_timing()
+            pc = e.path_counts()
+            total = pc["register_scatters"] + pc["atomic_scatters"]
+            results.append({"cluster_size": cs, "resort_interval": ri,
+                            "ms_per_substep": (kt["step_ms"] + kt["sort_ms"]) / steps,
+                            "atomic_scatter_fraction": pc["atomic_scatters"] / max(total, 1)})
+        finally:
+            e.close()
+    ok = [r for r in results if "ms_per_substep" in r]
+    if not ok:
+        raise RuntimeError("no batched configuration could run on this device")
+    best = min(ok, key=lambda r: r["ms_per_substep"])
+    return {"cluster_size": best["cluster_size"], "resort_interval": best["resort_interval"]}, results

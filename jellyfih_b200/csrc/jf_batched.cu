@@ -58,7 +58,7 @@ struct ChunkArgs {
   int32_t M;
   int32_t CS;
   int32_t K;                // substeps in this chunk
-  float t0;
+  const float* t_dev;       // sim_time at the chunk's start (device scalar)
   float dt;
   int32_t do_glow;
   unsigned long long* path;  // [register scatters, generic scatters, generic gathers]
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     oor_end = cend[cells];
   }
 
-  float t = a.t0;
+  float t = *a.t_dev;
   for (int s = 0; s <= a.K; ++s) {
     const bool do_g2p = s > 0;
     const bool do_p2g = s < a.K;
@@ -560,6 +560,13 @@ __global__ void dead_glow_kernel(const JfInst* __restrict__ inst, const int32_t*
   }
 }
 
+// sim_time += dt, K times, as the FP32 running sum of mpm_sim.py:340
+__global__ void advance_time_kernel(float* t, int K, float dt) {
+  float v = *t;
+  for (int s = 0; s < K; ++s) v = v + dt;
+  *t = v;
+}
+
 }  // namespace
 
 size_t jf_batched_smem_bytes(const jf_engine* e) {
@@ -567,7 +574,7 @@ size_t jf_batched_smem_bytes(const jf_engine* e) {
 }
 
 cudaError_t jf_batched_sort(jf_engine* e) {
-  JfTimed timed(e, true);
+  JfTimed timed(e, true, e->capturing);
   const int stride = e->max_cells + 2;
   cudaError_t err = cudaMemsetAsync(e->d_counts, 0, sizeof(int32_t) * (size_t)stride * e->M, e->stream);
   if (err != cudaSuccess) return err;
@@ -609,7 +616,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.M = e->M;
   a.CS = e->cluster;
   a.K = K;
-  a.t0 = e->t;
+  a.t_dev = e->d_time;
   a.dt = (float)e->dt;
   a.do_glow = (e->flags & JF_FLAG_GLOW) ? 1 : 0;
   a.path = e->d_path;
@@ -628,7 +635,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   cfg.numAttrs = 1;
   cudaError_t err;
   {
-    JfTimed timed(e, false);
+    JfTimed timed(e, false, e->capturing);
     err = cudaLaunchKernelEx(&cfg, chunk_kernel, a);
   }
   e->launches += 1;
@@ -668,19 +675,73 @@ int jf_batched_max_active_clusters(jf_engine* e, int cluster, int* out) {
   return (int)cudaOccupancyMaxActiveClusters(out, chunk_kernel, &cfg);
 }
 
+static cudaError_t chunk_with_sort(jf_engine* e, int K) {
+  cudaError_t err = jf_batched_sort(e);
+  if (err != cudaSuccess) return err;
+  if ((err = launch_chunk(e, K)) != cudaSuccess) return err;
+  advance_time_kernel<<<1, 1, 0, e->stream>>>(e->d_time, K, (float)e->dt);
+  e->launches += 1;
+  e->sorted = false;  // particles moved: re-sort before the next chunk
+  return cudaGetLastError();
+}
+
+// A graph of two (sort, chunk) pairs: two re-sorts swap the ping-pong particle
+// buffers twice, so the graph leaves them as it found them and can be replayed.
+static cudaError_t capture_pair(jf_engine* e, int K) {
+  if (e->graph_exec) {
+    cudaGraphExecDestroy(e->graph_exec);
+    e->graph_exec = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  const int64_t launches = e->launches;
+  cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return err;
+  e->capturing = true;
+  cudaError_t e1 = chunk_with_sort(e, K);
+  cudaError_t e2 = (e1 == cudaSuccess) ? chunk_with_sort(e, K) : e1;
+  e->capturing = false;
+  err = cudaStreamEndCapture(e->stream, &graph);
+  e->launches = launches;  // nothing ran yet
+  if (e2 != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return e2;
+  }
+  if (err != cudaSuccess) return err;
+  err = cudaGraphInstantiate(&e->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (err != cudaSuccess) return err;
+  e->graph_K = K;
+  e->graph_p = e->p.xv;
+  e->graph_launches = 2 * (e->max_slots > 0 ? 5 : 3) + ((e->flags & JF_FLAG_GLOW) ? 2 : 0);
+  return cudaSuccess;
+}
+
 cudaError_t jf_batched_step(jf_engine* e, int64_t n_steps) {
   const float dtf = (float)e->dt;
+  cudaError_t err = cudaMemcpyAsync(e->d_time, &e->t, sizeof(float), cudaMemcpyHostToDevice, e->stream);
+  if (err != cudaSuccess) return err;
+  const int R = e->resort_interval;
   while (n_steps > 0) {
-    if (!e->sorted) {
-      cudaError_t err = jf_batched_sort(e);
-      if (err != cudaSuccess) return err;
+    // graphs are replayed only when per-kernel timing is off (events cannot
+    // attribute time inside a replayed graph)
+    if (e->use_graphs && !e->timing && n_steps >= 2 * R) {
+      if (!e->graph_exec || e->graph_K != R || e->graph_p != e->p.xv) {
+        if ((err = capture_pair(e, R)) != cudaSuccess) return err;
+      }
+      {
+        JfTimed timed(e, false);
+        if ((err = cudaGraphLaunch(e->graph_exec, e->stream)) != cudaSuccess) return err;
+      }
+      e->launches += e->graph_launches;
+      for (int s = 0; s < 2 * R; ++s) e->t = e->t + dtf;
+      n_steps -= 2 * R;
+      continue;
     }
-    const int K = (int)(n_steps < e->resort_interval ? n_steps : e->resort_interval);
-    cudaError_t err = launch_chunk(e, K);
-    if (err != cudaSuccess) return err;
+    const int K = (int)(n_steps < R ? n_steps : R);
+    if ((err = chunk_with_sort(e, K)) != cudaSuccess) return err;
     for (int s = 0; s < K; ++s) e->t = e->t + dtf;
     n_steps -= K;
-    e->sorted = false;  // particles moved: re-sort before the next chunk
   }
+  // the host's copy is the authoritative time; the device copy keeps up with it
   return cudaSuccess;
 }

@@ -194,15 +194,16 @@ static cudaEvent_t pool_event(jf_engine* e) {
   return ev;
 }
 
-JfTimed::JfTimed(jf_engine* eng, bool sort) : e(eng), list(sort ? &eng->sort_events : &eng->step_events) {
-  if (!e->timing) return;
+JfTimed::JfTimed(jf_engine* eng, bool sort, bool skip)
+    : e(eng), list(sort ? &eng->sort_events : &eng->step_events), off(skip) {
+  if (!e->timing || off) return;
   a = pool_event(e);
   b = pool_event(e);
   cudaEventRecord(a, e->stream);
 }
 
 JfTimed::~JfTimed() {
-  if (!e->timing || !a) return;
+  if (!e->timing || off || !a) return;
   cudaEventRecord(b, e->stream);
   list->push_back({a, b});
 }
@@ -236,6 +237,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   e->flags = cfg->flags;
   e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 64;
   e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
+  e->use_graphs = (cfg->flags & JF_FLAG_NO_GRAPHS) == 0;
   auto bail = [&](int code, const std::string& msg) {
     jf_set_global_error(msg);
     jf_destroy(e);
@@ -258,7 +260,10 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
 
   // cluster size: grow while the launch still fits the SMs and bands keep >= 8 rows
   e->cluster = 4;
-  if (e->path == JF_PATH_BATCHED) {
+  if (cfg->cluster_size > 0) {
+    if (cfg->cluster_size > 16) return bail(JF_ERR_INVALID, "cluster_size must be <= 16");
+    e->cluster = cfg->cluster_size;
+  } else if (e->path == JF_PATH_BATCHED) {
     while (e->cluster < 16 && (int64_t)e->M * e->cluster * 2 <= n_sm &&
            (ny_max + e->cluster * 2 - 1) / (e->cluster * 2) >= 8)
       e->cluster *= 2;
@@ -327,6 +332,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
         (err = alloc(&e->d_counts, (size_t)(e->max_cells + 2) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_path, 4)) != cudaSuccess ||
+        (err = alloc(&e->d_time, 1)) != cudaSuccess ||
         (err = cudaMemset(e->d_path, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
       return bail(JF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
     if ((err = jf_batched_prepare(e)) != cudaSuccess)
@@ -366,7 +372,8 @@ int jf_destroy(jf_engine* e) {
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_band); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
-  cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i);
+  cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
   for (auto& pr : e->step_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto& pr : e->sort_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto ev : e->event_pool) cudaEventDestroy(ev);

@@ -66,6 +66,13 @@ struct jf_engine {
   int32_t* d_fit_i = nullptr;      // fitness staging: M muscle counts
 
   bool sorted = false;             // batched path: particle order valid for the current state
+  float* d_time = nullptr;         // batched path: sim_time on the device (chunk start)
+  bool use_graphs = true;          // batched path: replay (sort, chunk) pairs as a CUDA graph
+  bool capturing = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  int32_t graph_K = 0;
+  float4* graph_p = nullptr;       // particle buffer the graph was captured with
+  int64_t graph_launches = 0;
   float t = 0.0f;                  // sim_time (FP32 running sum, mpm_sim.py:340)
   int64_t launches = 0;            // kernels launched by this engine
   std::string err;
@@ -80,12 +87,14 @@ struct jf_engine {
   int64_t step_launches = 0, sort_launches = 0;
 };
 
-// Event pair bracketing one timed region (no-op when timing is off).
+// Event pair bracketing one timed region (no-op when timing is off or when
+// the work is being captured into a graph).
 struct JfTimed {
   jf_engine* e;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* list;
   cudaEvent_t a = nullptr, b = nullptr;
-  JfTimed(jf_engine* eng, bool sort);
+  bool off = false;
+  JfTimed(jf_engine* eng, bool sort, bool skip = false);
   ~JfTimed();
 };
 

@@ -47,21 +47,24 @@ class Engine:
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
-                 block_threads: int = 512):
+                 block_threads: int = 512, cluster_size: int = 0, graphs: bool = True):
         self._lib = L.load()
         self.instances = list(instances)
         self.M = len(self.instances)
         self.path = path
         descs = (L.JfInstanceDesc * self.M)(*[
             L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
+        flags = (L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
         cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
-                         L.JF_FLAG_GLOW if glow else 0, device, resort_interval, block_threads)
+                         flags, device, resort_interval, block_threads, cluster_size)
         h = L._E()
         rc = self._lib.jf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != L.JF_OK:
             raise L.JfError(rc, self._lib.jf_last_error(None).decode())
         self._h = h
         self.dt = dt
+        self.config = dict(path=path, resort_interval=resort_interval, block_threads=block_threads,
+                           cluster_size=cluster_size, graphs=graphs)
 
     # -- plumbing --------------------------------------------------------
     def _check(self, rc):

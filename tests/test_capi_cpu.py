@@ -45,11 +45,11 @@ def test_version(lib):
 
 def test_create_rejects_bad_config_before_touching_the_device(lib):
     h = L._E()
-    cfg = L.JfConfig(0, None, 2e-5, 0, 0, 0, 0, 0)
+    cfg = L.JfConfig(0, None, 2e-5, 0, 0, 0, 0, 0, 0)
     assert lib.jf_create(ctypes.byref(cfg), ctypes.byref(h)) == L.JF_ERR_INVALID
     assert b"n_instances" in lib.jf_last_error(None)
     descs = (L.JfInstanceDesc * 1)(L.JfInstanceDesc(10, 128, 128, 1.0))
-    cfg = L.JfConfig(1, descs, 2e-5, 7, 0, 0, 0, 0)
+    cfg = L.JfConfig(1, descs, 2e-5, 7, 0, 0, 0, 0, 0)
     assert lib.jf_create(ctypes.byref(cfg), ctypes.byref(h)) == L.JF_ERR_INVALID
     assert lib.jf_create(None, ctypes.byref(h)) == L.JF_ERR_INVALID
 

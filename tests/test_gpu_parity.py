@@ -302,3 +302,35 @@ def test_gpu_fitness_matches_host_restatement():
         np.testing.assert_allclose(got[valid], ref[valid], rtol=1e-15)
         assert np.all(got[~valid] == got[valid].max() + 1.0)
     e.close()
+
+
+def test_graph_replay_matches_direct_launches():
+    """Chunks replayed from a CUDA graph give the direct launches' results."""
+    from jellyfih_b200 import InstanceSpec
+    pos, mat, fib, st, c, f = _tank_instance(51, n_slots=20000, grid=64, ny=64)
+    outs = []
+    for graphs in (True, False):
+        e = _engine([InstanceSpec(20000, 64, 64, 1.0)] * 3, "batched", resort_interval=8, graphs=graphs)
+        for m in range(3):
+            e.load(m, pos, mat, fib)
+        e.set_params(contraction=[c] * 3, freq=[f] * 3)
+        e.step(8 * 2 * 3 + 5)   # three graph replays plus a direct remainder
+        assert e.time == np.float32(e.time)
+        outs.append((e.read(0), e.time, e.run_headless(40)))
+        e.close()
+    (a, ta, ra), (b, tb, rb) = outs
+    assert ta == tb
+    live = mat >= 0
+    assert np.abs(a["x"][live] - b["x"][live]).max() < 1e-5
+    assert_norm_close(a["v"][live], b["v"][live], 1e-3, "graph v")
+    np.testing.assert_allclose(ra, rb, rtol=1e-5)
+
+
+def test_autotuner_runs_and_picks_a_valid_config():
+    from jellyfih_b200 import InstanceSpec
+    from jellyfih_b200.autotune import autotune
+    pos, mat, fib, st, c, f = _tank_instance(52, n_slots=20000, grid=64, ny=64)
+    best, table = autotune([InstanceSpec(20000, 64, 64, 1.0)] * 4, [(pos, mat, fib)] * 4,
+                           clusters=(0, 4), resorts=(8, 32), trial_steps=64)
+    assert best["resort_interval"] in (8, 32)
+    assert any("ms_per_substep" in r for r in table)

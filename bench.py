@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--resort", type=int, default=64)
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     return ap.parse_args()
 
 
@@ -168,6 +169,60 @@ def cpu_baseline(inputs, target_s=12.0):
             "kind": "port",
             "sample": f"{len(inputs)} instances x {n} substeps of the same workload on the CPU oracle "
                       f"({el:.1f} s)"}
+
+
+def uneven_inputs(seed=3000):
+    """48 instances on 128^2 with 40K-120K live particles (lattice spacing
+    dx/k, k seeded in [1.6, 2.7]) and 16 tall tanks 128x256 (domain height 2,
+    spawn (0.5, 0.6), ~126K live of 160K slots); genomes uniform in bounds."""
+    from jellyfih_b200 import InstanceSpec, tank
+    rng = np.random.default_rng(seed)
+    genomes = tank.uniform_genomes(64, seed)
+    specs, data = [], []
+    for m, g in enumerate(genomes):
+        c, f = tank.timing_params(g)
+        if m < 48:
+            k = float(rng.uniform(1.6, 2.7))
+            pos, mat, fib, st = tank.fill_tank(g, 120000, spacing_div=k)
+            specs.append(InstanceSpec(120000, 128, 128, 1.0))
+        else:
+            pos, mat, fib, st = tank.fill_tank(g, 160000, domain_height=2.0, spawn_offset=tank.TALL_SPAWN)
+            specs.append(InstanceSpec(160000, 128, 256, 2.0))
+        data.append((pos, mat, fib, c, f, st))
+    return specs, data
+
+
+def uneven_leg(device, stream, substeps=256):
+    """Particle-steps/s of the uneven batch in one batched launch per chunk,
+    CUDA-graph replay on, for re-sort intervals 1, 4, 16 and the autotuned
+    configuration."""
+    import torch
+    from jellyfih_b200 import Engine
+    from jellyfih_b200.autotune import autotune
+    specs, data = uneven_inputs()
+    live = sum(int((d[1] >= 0).sum()) for d in data)
+    out = {"instances": len(specs), "live_particles": live, "substeps": substeps, "resort": {}}
+
+    def timed(ri, cs=0):
+        e = Engine(specs, path="batched", device=device, resort_interval=ri, cluster_size=cs)
+        e.set_stream(stream)
+        load_all(e, data)
+        e.step(2 * ri)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.step(substeps)
+        ev1.record(stream)
+        ev1.synchronize()
+        e.close()
+        return live * substeps / (ev0.elapsed_time(ev1) / 1e3)
+
+    for ri in (1, 4, 16):
+        out["resort"][str(ri)] = timed(ri)
+    best, table = autotune(specs, [d[:3] for d in data], clusters=(0, 8), resorts=(16, 32, 64),
+                           trial_steps=64, device=device)
+    out["autotuned"] = dict(best, value=timed(best["resort_interval"], best["cluster_size"]))
+    out["unit"] = UNIT
+    return out
 
 
 def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
@@ -384,6 +439,24 @@ def run_ours(args):
                            "batched_over_plain": value / plain_value}
 
         extras["differentiable"] = grad_leg(inputs[:8], local, stream)
+
+        # the same workload with (sort, chunk) pairs replayed from a CUDA graph
+        g = Engine([spec] * M, path="batched", device=local, resort_interval=args.resort,
+                   block_threads=args.block, graphs=True)
+        g.set_stream(stream)
+        load_all(g, inputs)
+        g.step(2 * args.resort)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(2):
+            g.step(S)
+        e1.record(stream)
+        e1.synchronize()
+        extras["graphs"] = {"value": live * 2 * S / (e0.elapsed_time(e1) / 1e3) * world, "unit": UNIT,
+                            "steps": 2, "note": "bench steps replayed as CUDA graphs, kernel timing off"}
+        g.close()
+        if not args.no_uneven:
+            extras["uneven"] = uneven_leg(local, stream)
 
         if rank == 0 and world == 1:
             extras["cpu_baseline"] = cpu_baseline(inputs)

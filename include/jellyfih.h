@@ -55,6 +55,9 @@ typedef struct {
   int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 64 */
   int32_t block_threads;                /* batched: threads per CTA, 0 = 512 */
   int32_t cluster_size;                 /* batched: CTAs per instance (1..16), 0 = automatic */
+  int32_t cell_cap;                     /* batched: particles a cell lane accumulates per substep;
+                                           the rest of the cell goes through per-particle atomics.
+                                           0 = chosen per instance at every re-sort, >= 16 = no cap */
 } jf_config;
 
 /* Engine life cycle.  Replaces the import-time allocation of mpm_sim.py:86-149;
@@ -160,10 +163,12 @@ int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m);
 int jf_error_flags(jf_engine* e, int32_t* out);
 int jf_clear_error_flags(jf_engine* e);
 
-/* Batched path counters since the last reset: out[0] particle scatters
- * accumulated in a lane's register block, out[1] scatters through per-particle
- * atomics (drifted or out-of-range particles), out[2] G2P gathers outside the
- * CTA's shared-memory window.  All zero on the plain path. */
+/* Batched path counters since the last reset (out has 4 entries): out[0]
+ * particle scatters accumulated in a lane's register block, out[1] scatters
+ * through per-particle atomics (drifted or out-of-range particles), out[2] G2P
+ * gathers outside the CTA's shared-memory window, out[3] particles beyond
+ * their cell's per-lane cap, handed to the CTA's balanced overflow pass
+ * (per-particle atomics).  All zero on the plain path. */
 int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset);
 
 /* Largest grid, in nodes (n_grid * n_grid_y), jf_substep_noalloc accepts. */

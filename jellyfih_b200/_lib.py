@@ -31,7 +31,8 @@ class JfConfig(ctypes.Structure):
     _fields_ = [("n_instances", ctypes.c_int32), ("instances", ctypes.POINTER(JfInstanceDesc)),
                 ("dt", ctypes.c_double), ("path", ctypes.c_int32), ("flags", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("resort_interval", ctypes.c_int32),
-                ("block_threads", ctypes.c_int32), ("cluster_size", ctypes.c_int32)]
+                ("block_threads", ctypes.c_int32), ("cluster_size", ctypes.c_int32),
+                ("cell_cap", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p

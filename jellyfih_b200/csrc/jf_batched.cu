@@ -27,6 +27,16 @@ constexpr int kHaloHi = 3;  // rows above: the stencil's +2 plus one row of drif
 constexpr int kHalo = kHaloLo + kHaloHi;
 constexpr int kSortThreads = 256;
 constexpr int kScanThreads = 1024;
+// Per-lane cap of a cell's particles: a warp's cell loop runs as many
+// iterations as its fullest cell, so the particles a cell holds beyond the
+// cap are listed per band at the re-sort and handled 32 at a time, one per
+// lane with per-particle atomics, as extra tasks of the band's task queue.
+// The cap is chosen per instance at each re-sort by the cost model
+// 32 * sum_warps min(max count, cap) + 1.5 * overflow (lane-iterations), over
+// caps 1 .. kCapCandidates - 1 and "no cap".
+constexpr int kCapCandidates = 16;
+constexpr int kMaxCluster = 16;
+constexpr int kNoCap = 1 << 30;
 
 // Sort cell of a particle: (floor(X - 1/4), floor(Y - 1/4)) in grid units,
 // clamped at 0.  The stencil base trunc(X - 1/2) of a particle in sort cell k
@@ -51,7 +61,10 @@ struct ChunkArgs {
   float* Jp;
   const float2* fiber;
   float* glow;
-  const int32_t* cell_end;  // M x stride: end of each cell's run (relative to p_off)
+  const int32_t* cell_start;  // M x stride: start of each bin's run (relative to p_off)
+  const int32_t* cap;         // M: particles a cell lane takes; the rest are overflow
+  const int32_t* ovlist;      // overflow positions (relative to p_off), grouped by band
+  const int32_t* ovband;      // M x (CS + 1): band starts in ovlist
   int32_t stride;
   float4* grid;             // grid of the chunk's last substep, node = g_off + j * nx + i
   int32_t* err;
@@ -61,7 +74,7 @@ struct ChunkArgs {
   const float* t_dev;       // sim_time at the chunk's start (device scalar)
   float dt;
   int32_t do_glow;
-  unsigned long long* path;  // [register scatters, generic scatters, generic gathers]
+  unsigned long long* path;  // [register scatters, generic scatters, generic gathers, overflow]
 };
 
 // Shared-memory window of one CTA: grid rows [win0, win0 + WR) of its
@@ -217,10 +230,11 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   w.Ax = w.Gy + WN;
   w.Ay = w.Ax + WN;
   w.Am = w.Ay + WN;
+  const int cap = a.cap[m];
   const int tid = threadIdx.x, nth = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, n_warps = nth >> 5;
   const int cells = nx * ny;
-  const int32_t* cend = a.cell_end + (int64_t)m * a.stride;
+  const int32_t* cstart = a.cell_start + (int64_t)m * a.stride;
   const int64_t p0 = I.p_off;
   // this instance's particle arrays, indexed by position within the instance
   float4* __restrict__ xv_m = a.xv + p0;
@@ -229,7 +243,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const int32_t* __restrict__ mat_m = a.mat + p0;
 
   for (int n = tid; n < 5 * WN; n += nth) sm[n] = 0.0f;
-  unsigned n_fast = 0, n_generic = 0, n_gather_generic = 0;
+  unsigned n_fast = 0, n_generic = 0, n_gather_generic = 0, n_overflow = 0;
   cluster.sync();
 
   // G2P of the previous substep, then P2G of this one, for a particle that
@@ -262,13 +276,20 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     }
   };
 
+  // tasks: 32-cell row segments of the band, then groups of 32 generic
+  // particles (this band's overflow list, then, in the last band, live
+  // particles outside every stencil range)
   const int segs = (nx + 31) >> 5;
-  const int n_tasks = max(own_hi - row0, 0) * segs;
-  int oor_beg = 0, oor_end = 0;
+  const int n_cell_tasks = max(own_hi - row0, 0) * segs;
+  const int32_t* ov = a.ovlist + p0 + a.ovband[m * (CS + 1) + r];
+  const int n_ov = a.ovband[m * (CS + 1) + r + 1] - a.ovband[m * (CS + 1) + r];
+  int oor_beg = 0, n_oor = 0;
   if (r == CS - 1) {
-    oor_beg = cend[cells - 1];
-    oor_end = cend[cells];
+    oor_beg = cstart[cells];
+    n_oor = cstart[cells + 1] - oor_beg;
   }
+  const int n_generic_all = n_ov + n_oor;
+  const int n_tasks = n_cell_tasks + ((n_generic_all + 31) >> 5);
 
   float t = *a.t_dev;
   for (int s = 0; s <= a.K; ++s) {
@@ -283,14 +304,27 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     if (tid == 0) s_next_task = n_warps;
     __syncthreads();
     for (int task = warp; task < n_tasks;) {
+      if (task >= n_cell_tasks) {
+        const int e = ((task - n_cell_tasks) << 5) + lane;
+        if (e < n_generic_all) {
+          const bool over = e < n_ov;
+          particle_generic(p0 + (over ? ov[e] : oor_beg + e - n_ov), do_g2p, do_p2g, pressure);
+          n_overflow += over ? 1u : 0u;
+          n_generic += over ? 0u : 1u;
+        }
+        int nt = 0;
+        if (lane == 0) nt = atomicAdd(&s_next_task, 1);
+        task = __shfl_sync(0xffffffffu, nt, 0);
+        continue;
+      }
       const int cy = row0 + task / segs;
       const int seg0 = (task % segs) << 5;
       const int cx = seg0 + lane;
       int beg = 0, end = 0;
       if (cx < nx) {
         const int c = cy * nx + cx;
-        end = cend[c];
-        beg = c > 0 ? cend[c - 1] : 0;
+        beg = cstart[c];
+        end = min(cstart[c + 1], beg + cap);  // the rest of the cell is overflow
       }
       // 4x4 node block: columns cx-1 .. cx+2, rows cy-1 .. cy+2
       float acc[48];
@@ -366,11 +400,6 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       if (lane == 0) nt = atomicAdd(&s_next_task, 1);
       task = __shfl_sync(0xffffffffu, nt, 0);
     }
-    // live particles outside every stencil range (last band only)
-    for (int k = oor_beg + tid; k < oor_end; k += nth) {
-      particle_generic(p0 + k, do_g2p, do_p2g, pressure);
-      ++n_generic;
-    }
     __syncthreads();
 
     if (do_p2g) {
@@ -430,10 +459,12 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     const unsigned f = __reduce_add_sync(0xffffffffu, n_fast);
     const unsigned g = __reduce_add_sync(0xffffffffu, n_generic);
     const unsigned h = __reduce_add_sync(0xffffffffu, n_gather_generic);
+    const unsigned o = __reduce_add_sync(0xffffffffu, n_overflow);
     if (lane == 0) {
       atomicAdd(a.path + 0, (unsigned long long)f);
       atomicAdd(a.path + 1, (unsigned long long)g);
       atomicAdd(a.path + 2, (unsigned long long)h);
+      atomicAdd(a.path + 3, (unsigned long long)o);
     }
   }
   // peers may still read this CTA's grid rows in their last G2P pass
@@ -444,7 +475,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
 // particles outside the stencil range and one for dead slots.
 __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* __restrict__ xv,
                                  const int32_t* __restrict__ mat, int32_t* __restrict__ keys,
-                                 int32_t* __restrict__ counts, int stride) {
+                                 int32_t* __restrict__ rank, int32_t* __restrict__ counts, int stride) {
   const int m = blockIdx.y;
   const JfInst I = inst[m];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -465,22 +496,71 @@ __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* 
     }
   }
   keys[g] = key;
-  atomicAdd(counts + (int64_t)m * stride + key, 1);
+  rank[g] = atomicAdd(counts + (int64_t)m * stride + key, 1);
 }
 
-// Exclusive scan of one instance's bins (counts become start cursors) and the
-// CTA band table: CTA r streams [band[r], band[r+1]); the last CTA also takes
-// the out-of-range bin.
+// Per instance: the cell cap, the exclusive scan of the bins (counts become
+// bin starts), the CTA band table (CTA r owns positions [band[r], band[r+1]);
+// the last CTA also takes the out-of-range bin) and the band starts and
+// cursors of the overflow list.
 __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* __restrict__ inst,
                                                                 int32_t* __restrict__ counts,
                                                                 int stride, int32_t* __restrict__ band,
-                                                                int CS) {
+                                                                int32_t* __restrict__ cap_out,
+                                                                int32_t* __restrict__ ovband,
+                                                                int32_t* __restrict__ ovcur, int CS,
+                                                                int fixed_cap) {
   __shared__ int warp_sums[kScanThreads / 32];
+  __shared__ int s_cost[kCapCandidates];
+  __shared__ int s_band_over[kMaxCluster][kCapCandidates];
   const int m = blockIdx.x;
   const JfInst I = inst[m];
   const int cells = I.nx * I.ny;
   const int nbins = cells + 2;
   int32_t* c = counts + (int64_t)m * stride;
+
+  // per-lane cap from the cell counts (candidate 0 = no cap); costs in
+  // quarter lane-iterations: 128 per warp iteration, 6 per overflow particle
+  if (threadIdx.x < kCapCandidates) s_cost[threadIdx.x] = 0;
+  for (int i = threadIdx.x; i < kMaxCluster * kCapCandidates; i += kScanThreads)
+    (&s_band_over[0][0])[i] = 0;
+  __syncthreads();
+  {
+    const int segs = (I.nx + 31) >> 5;
+    for (int sg = threadIdx.x; sg < I.ny * segs; sg += kScanThreads) {
+      const int row = sg / segs;
+      const int x0 = (sg - row * segs) << 5;
+      const int xn = min(32, I.nx - x0);
+      const int32_t* cr = c + row * I.nx + x0;
+      int mx = 0;
+      for (int i = 0; i < xn; ++i) mx = max(mx, cr[i]);
+      if (mx == 0) continue;
+      const int br = min(row / I.band_h, CS - 1);
+      atomicAdd(&s_cost[0], 128 * mx);
+      for (int k = 1; k < kCapCandidates; ++k) {
+        int ov = 0;
+        if (k < mx)
+          for (int i = 0; i < xn; ++i) ov += max(0, cr[i] - k);
+        atomicAdd(&s_cost[k], 128 * min(mx, k) + 6 * ov);
+        if (ov) atomicAdd(&s_band_over[br][k], ov);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int best = 0;
+    for (int k = 1; k < kCapCandidates; ++k)
+      if (s_cost[k] < s_cost[best]) best = k;
+    if (fixed_cap > 0) best = fixed_cap < kCapCandidates ? fixed_cap : 0;
+    cap_out[m] = best == 0 ? kNoCap : best;
+    int run = 0;
+    for (int r = 0; r < CS; ++r) {
+      ovband[m * (CS + 1) + r] = run;
+      ovcur[m * CS + r] = run;
+      run += best == 0 ? 0 : s_band_over[r][best];
+    }
+    ovband[m * (CS + 1) + CS] = run;
+  }
   const int per = (nbins + kScanThreads - 1) / kScanThreads;
   const int b0 = threadIdx.x * per;
   const int b1 = min(b0 + per, nbins);
@@ -523,16 +603,26 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
   }
 }
 
+// Moves every particle to bin start + rank; particles of a cell beyond the
+// cap are also listed in their band's part of the overflow list.
 __global__ void sort_scatter_kernel(const JfInst* __restrict__ inst, const int32_t* __restrict__ keys,
-                                    int32_t* __restrict__ counts, int stride, JfParticles src,
-                                    JfParticles dst) {
+                                    const int32_t* __restrict__ rank, const int32_t* __restrict__ starts,
+                                    int stride, const int32_t* __restrict__ cap, int CS,
+                                    int32_t* __restrict__ ovcur, int32_t* __restrict__ ovlist,
+                                    JfParticles src, JfParticles dst) {
   const int m = blockIdx.y;
   const JfInst I = inst[m];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= I.n_slots) return;
   const int64_t g = I.p_off + k;
   const int key = keys[g];
-  const int64_t d = I.p_off + atomicAdd(counts + (int64_t)m * stride + key, 1);
+  const int rk = rank[g];
+  const int32_t rel = starts[(int64_t)m * stride + key] + rk;
+  const int64_t d = I.p_off + rel;
+  if (key < I.nx * I.ny && rk >= cap[m]) {
+    const int band = min((key / I.nx) / I.band_h, CS - 1);
+    ovlist[I.p_off + atomicAdd(ovcur + m * CS + band, 1)] = rel;
+  }
   dst.xv[d] = src.xv[g];
   dst.C[d] = src.C[g];
   dst.F[d] = src.F[g];
@@ -581,13 +671,15 @@ cudaError_t jf_batched_sort(jf_engine* e) {
   const dim3 grid((e->max_slots + kSortThreads - 1) / kSortThreads, e->M);
   if (e->max_slots > 0) {
     sort_keys_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->p.xv, e->p.mat, e->d_keys,
-                                                          e->d_counts, stride);
+                                                          e->d_rank, e->d_counts, stride);
   }
   sort_scan_kernel<<<e->M, kScanThreads, 0, e->stream>>>(e->d_inst, e->d_counts, stride, e->d_band,
-                                                         e->cluster);
+                                                         e->d_cap, e->d_ovband, e->d_ovcur, e->cluster,
+                                                         e->cell_cap);
   if (e->max_slots > 0) {
-    sort_scatter_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->d_keys, e->d_counts, stride,
-                                                             e->p, e->q);
+    sort_scatter_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->d_keys, e->d_rank, e->d_counts,
+                                                             stride, e->d_cap, e->cluster, e->d_ovcur,
+                                                             e->d_ovlist, e->p, e->q);
   }
   e->launches += (e->max_slots > 0) ? 3 : 1;
   err = cudaGetLastError();
@@ -609,7 +701,10 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.Jp = e->p.Jp;
   a.fiber = e->p.fiber;
   a.glow = e->p.glow;
-  a.cell_end = e->d_counts;
+  a.cell_start = e->d_counts;
+  a.cap = e->d_cap;
+  a.ovlist = e->d_ovlist;
+  a.ovband = e->d_ovband;
   a.stride = e->max_cells + 2;
   a.grid = e->d_grid;
   a.err = e->d_err;

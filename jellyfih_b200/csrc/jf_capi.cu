@@ -237,12 +237,14 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   e->flags = cfg->flags;
   e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 64;
   e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
+  e->cell_cap = cfg->cell_cap;
   e->use_graphs = (cfg->flags & JF_FLAG_NO_GRAPHS) == 0;
   auto bail = [&](int code, const std::string& msg) {
     jf_set_global_error(msg);
     jf_destroy(e);
     return code;
   };
+  if (cfg->cell_cap < 0) return bail(JF_ERR_INVALID, "cell_cap must be >= 0");
   if (e->block_threads > 512 || e->block_threads % 32) return bail(JF_ERR_INVALID, "block_threads must be a multiple of 32, <= 512");
 
   int ny_max = 0;
@@ -329,8 +331,13 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   if (e->path == JF_PATH_BATCHED) {
     if ((err = alloc_particles(e->q, p_off)) != cudaSuccess ||
         (err = alloc(&e->d_keys, p_off)) != cudaSuccess ||
+        (err = alloc(&e->d_rank, p_off)) != cudaSuccess ||
+        (err = alloc(&e->d_ovlist, p_off)) != cudaSuccess ||
+        (err = alloc(&e->d_ovband, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_ovcur, (size_t)e->cluster * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_counts, (size_t)(e->max_cells + 2) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_cap, e->M)) != cudaSuccess ||
         (err = alloc(&e->d_path, 4)) != cudaSuccess ||
         (err = alloc(&e->d_time, 1)) != cudaSuccess ||
         (err = cudaMemset(e->d_path, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
@@ -370,7 +377,8 @@ int jf_destroy(jf_engine* e) {
   free_particles(e->p);
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
-  cudaFree(e->d_band); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
+  cudaFree(e->d_rank); cudaFree(e->d_ovlist); cudaFree(e->d_ovband); cudaFree(e->d_ovcur);
+  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
@@ -706,14 +714,14 @@ int64_t jf_kernel_launches(const jf_engine* e) { return e ? e->launches : -1; }
 
 int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset) {
   if (check_engine(e) || !out) return JF_ERR_INVALID;
-  out[0] = out[1] = out[2] = 0;
+  out[0] = out[1] = out[2] = out[3] = 0;
   if (!e->d_path) return JF_OK;
   int rc = set_device(e);
   if (rc) return rc;
   unsigned long long h[4] = {0, 0, 0, 0};
   JF_CK(cudaMemcpyAsync(h, e->d_path, sizeof(h), cudaMemcpyDeviceToHost, e->stream), "read path counters");
   JF_CK(cudaStreamSynchronize(e->stream), "path counters sync");
-  for (int i = 0; i < 3; ++i) out[i] = (int64_t)h[i];
+  for (int i = 0; i < 4; ++i) out[i] = (int64_t)h[i];
   if (reset) JF_CK(cudaMemsetAsync(e->d_path, 0, sizeof(h), e->stream), "reset path counters");
   return JF_OK;
 }

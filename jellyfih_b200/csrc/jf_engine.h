@@ -53,8 +53,14 @@ struct jf_engine {
   JfParticles p;                   // live buffers
   JfParticles q;                   // batched path: sort destination
   int32_t* d_keys = nullptr;       // batched path: cell key per engine position
-  int32_t* d_counts = nullptr;     // batched path: M x (max_cells + 2) histogram / cursors
+  int32_t* d_rank = nullptr;       // batched path: rank of the particle within its cell
+  int32_t* d_counts = nullptr;     // batched path: M x (max_cells + 2) histogram, then bin starts
+  int32_t* d_ovlist = nullptr;     // batched path: per band, sorted positions beyond the cell cap
+  int32_t* d_ovband = nullptr;     // batched path: M x (cluster + 1) overflow list band starts
+  int32_t* d_ovcur = nullptr;      // batched path: M x cluster overflow list cursors
   int32_t* d_band = nullptr;       // batched path: M x (cluster + 1) particle ranges
+  int32_t* d_cap = nullptr;        // batched path: per-instance particles per cell lane
+  int32_t cell_cap = 0;            // batched path: fixed cell cap, 0 = cost model per re-sort
   float4* d_grid = nullptr;        // grid nodes (node = g_off + j * nx + i): (v0, v1, m, 0)
   double* d_stats = nullptr;       // M x 6 CoM sums (payload y, count, x; body y, count, x)
   int32_t* d_err = nullptr;        // per-instance non-finite flags

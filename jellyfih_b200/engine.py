@@ -47,7 +47,8 @@ class Engine:
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
-                 block_threads: int = 512, cluster_size: int = 0, graphs: bool = True):
+                 block_threads: int = 512, cluster_size: int = 0, graphs: bool = True,
+                 cell_cap: int = 0):
         self._lib = L.load()
         self.instances = list(instances)
         self.M = len(self.instances)
@@ -56,7 +57,7 @@ class Engine:
             L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
         flags = (L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
         cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
-                         flags, device, resort_interval, block_threads, cluster_size)
+                         flags, device, resort_interval, block_threads, cluster_size, cell_cap)
         h = L._E()
         rc = self._lib.jf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != L.JF_OK:
@@ -64,7 +65,7 @@ class Engine:
         self._h = h
         self.dt = dt
         self.config = dict(path=path, resort_interval=resort_interval, block_threads=block_threads,
-                           cluster_size=cluster_size, graphs=graphs)
+                           cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap)
 
     # -- plumbing --------------------------------------------------------
     def _check(self, rc):
@@ -105,12 +106,13 @@ class Engine:
                 "sort_launches": ol.value}
 
     def path_counts(self, reset: bool = False) -> dict:
-        """Batched path counters: register-block scatters, per-particle scatters,
-        gathers outside the CTA window."""
-        out = np.zeros(3, np.int64)
+        """Batched path counters: register-block scatters, per-particle scatters
+        of drifted particles, gathers outside the CTA window, and particles
+        beyond their cell lane's cap (scattered in the CTA's overflow pass)."""
+        out = np.zeros(4, np.int64)
         self._check(self._lib.jf_path_counts(self._h, _ptr(out), 1 if reset else 0))
         return {"register_scatters": int(out[0]), "atomic_scatters": int(out[1]),
-                "remote_gathers": int(out[2])}
+                "remote_gathers": int(out[2]), "overflow_scatters": int(out[3])}
 
     def set_stream(self, stream) -> None:
         """Queue work on ``stream`` (a cudaStream_t as int, or a torch.cuda.Stream)."""

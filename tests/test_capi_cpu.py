@@ -65,4 +65,4 @@ def test_null_handle_calls_fail_cleanly(lib):
 def test_struct_layout():
     assert ctypes.sizeof(L.JfInstanceDesc) == 16
     assert L.JfConfig.instances.offset == 8 and L.JfConfig.dt.offset == 16
-    assert ctypes.sizeof(L.JfConfig) == 48
+    assert ctypes.sizeof(L.JfConfig) == 56

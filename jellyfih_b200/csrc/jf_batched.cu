@@ -276,9 +276,12 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     }
   };
 
-  // tasks: 32-cell row segments of the band, then groups of 32 generic
-  // particles (this band's overflow list, then, in the last band, live
-  // particles outside every stencil range)
+  // tasks: groups of 32 generic particles (this band's overflow list, then,
+  // in the last band, live particles outside every stencil range), then the
+  // 32-cell row segments of the band.  The slower generic groups go first so
+  // that the segments even out the end of the pass; a group's lanes take
+  // entries n_gen_tasks apart, far apart in the list, so that their atomics
+  // rarely meet on one node.
   const int segs = (nx + 31) >> 5;
   const int n_cell_tasks = max(own_hi - row0, 0) * segs;
   const int32_t* ov = a.ovlist + p0 + a.ovband[m * (CS + 1) + r];
@@ -289,7 +292,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     n_oor = cstart[cells + 1] - oor_beg;
   }
   const int n_generic_all = n_ov + n_oor;
-  const int n_tasks = n_cell_tasks + ((n_generic_all + 31) >> 5);
+  const int n_gen_tasks = (n_generic_all + 31) >> 5;
+  const int n_tasks = n_cell_tasks + n_gen_tasks;
 
   float t = *a.t_dev;
   for (int s = 0; s <= a.K; ++s) {
@@ -303,9 +307,9 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     // claim row segments from a shared counter so that they finish together
     if (tid == 0) s_next_task = n_warps;
     __syncthreads();
-    for (int task = warp; task < n_tasks;) {
-      if (task >= n_cell_tasks) {
-        const int e = ((task - n_cell_tasks) << 5) + lane;
+    for (int task_id = warp; task_id < n_tasks;) {
+      if (task_id < n_gen_tasks) {
+        const int e = task_id + lane * n_gen_tasks;
         if (e < n_generic_all) {
           const bool over = e < n_ov;
           particle_generic(p0 + (over ? ov[e] : oor_beg + e - n_ov), do_g2p, do_p2g, pressure);
@@ -314,9 +318,10 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         }
         int nt = 0;
         if (lane == 0) nt = atomicAdd(&s_next_task, 1);
-        task = __shfl_sync(0xffffffffu, nt, 0);
+        task_id = __shfl_sync(0xffffffffu, nt, 0);
         continue;
       }
+      const int task = task_id - n_gen_tasks;
       const int cy = row0 + task / segs;
       const int seg0 = (task % segs) << 5;
       const int cx = seg0 + lane;
@@ -330,31 +335,31 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       float acc[48];
 #pragma unroll
       for (int q = 0; q < 48; ++q) acc[q] = 0.0f;
-      float4 nxv, nC, nF;
+      float4 nxv;
       int nmt = -1;
       if (beg < end) {
         nxv = xv_m[beg];
-        nC = C_m[beg];
         nmt = mat_m[beg];
-        nF = F_m[beg];
       }
       for (int k = beg; k < end; ++k) {
         const float4 xv = nxv;
-        float4 C = nC;
-        float4 F = nF;
         const int mt = nmt;
+        float4 F = F_m[k];  // first used by P2G, after the gather
         if (k + 1 < end) {  // next particle of this cell, loaded while this one computes
           nxv = xv_m[k + 1];
-          nC = C_m[k + 1];
           nmt = mat_m[k + 1];
-          nF = F_m[k + 1];
         }
         float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
         float jp = 1.0f;
         if (mt == 2 || a.do_glow) jp = a.Jp[p0 + k];
+        // G2P replaces v and C from the grid (mpm_sim.py:315-327); the stored
+        // C is read only where G2P does not run
+        float4 C;
         if (do_g2p) {
           JfStencil st;
-          if (jf_stencil(I, x, st)) {
+          if (!jf_stencil(I, x, st)) {
+            C = C_m[k];
+          } else {
             const int wr0 = st.by - w.win0;
             if (wr0 >= 0 && wr0 + 2 < w.WR) {
               const int wb = wr0 * nx + st.bx;
@@ -373,6 +378,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
           xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
           C_m[k] = C;
+        } else {
+          C = C_m[k];
         }
         if (do_p2g) {
           JfStencil st;
@@ -398,7 +405,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       if (do_p2g) flush_block(acc, w, lane, cx, cy, seg0, nx);
       int nt = 0;
       if (lane == 0) nt = atomicAdd(&s_next_task, 1);
-      task = __shfl_sync(0xffffffffu, nt, 0);
+      task_id = __shfl_sync(0xffffffffu, nt, 0);
     }
     __syncthreads();
 

@@ -91,18 +91,25 @@ __host__ __device__ inline float jf_activation(float freq, float contraction, fl
 
 // 2x2 SVD as taichi 1.7.4 ti.svd computes it (_svd2d): polar decomposition
 // A = R S with R = [[c,-s],[s,c]] from (A00 + A11, A10 - A01), one Jacobi
-// rotation of S unless |S01| < 1e-5, singular values ordered s1 >= s2 with
-// the matching V, U = R V.  Matrices row-major in float4 (00, 01, 10, 11).
-__device__ __forceinline__ void jf_svd2(float4 A, float4& U, float2& sig, float4& V) {
+// rotation (cc, ss) of S unless |S01| < 1e-5, singular values ordered
+// s1 >= s2 with the matching V, U = R V.  Matrices row-major in float4
+// (00, 01, 10, 11).  jf_svd2_values stops before the ordering: it returns the
+// rotations and the two singular values in Jacobi order.
+struct JfSvdRot {
+  float c, s, cc, ss, s1, s2;
+};
+
+__device__ __forceinline__ JfSvdRot jf_svd2_values(float4 A) {
+  JfSvdRot o;
   const float x = radd(A.x, A.w);
   const float y = rsub(A.z, A.y);
   const float scale = 1.0f / sqrtf(radd(rmul(x, x), rmul(y, y)));
-  const float c = rmul(x, scale);
-  const float s = rmul(y, scale);
-  const float ms = -s;
-  const float S00 = rdot2(c, A.x, s, A.z);
-  const float S01 = rdot2(c, A.y, s, A.w);
-  const float S11 = rdot2(ms, A.y, c, A.w);
+  o.c = rmul(x, scale);
+  o.s = rmul(y, scale);
+  const float ms = -o.s;
+  const float S00 = rdot2(o.c, A.x, o.s, A.z);
+  const float S01 = rdot2(o.c, A.y, o.s, A.w);
+  const float S11 = rdot2(ms, A.y, o.c, A.w);
   // Both branches of the reference's |S01| < 1e-5 test are evaluated and the
   // result selected, so lanes of a warp do not diverge; the selected values
   // are those of the taken branch (the other one may be NaN and is dropped).
@@ -116,10 +123,16 @@ __device__ __forceinline__ void jf_svd2(float4 A, float4& U, float2& sig, float4
   const float j1 = radd(rsub(rmul(cc2, S00), rmul(cs2, S01)), rmul(ss2, S11));
   const float j2 = radd(radd(rmul(ss2, S00), rmul(cs2, S01)), rmul(cc2, S11));
   const bool diagonal = fabsf(S01) < 1e-5f;
-  const float cc = diagonal ? 1.0f : jc;
-  const float ss = diagonal ? 0.0f : js;
-  float s1 = diagonal ? S00 : j1;
-  float s2 = diagonal ? S11 : j2;
+  o.cc = diagonal ? 1.0f : jc;
+  o.ss = diagonal ? 0.0f : js;
+  o.s1 = diagonal ? S00 : j1;
+  o.s2 = diagonal ? S11 : j2;
+  return o;
+}
+
+__device__ __forceinline__ void jf_svd2_vectors(const JfSvdRot& r, float4& U, float2& sig, float4& V) {
+  float s1 = r.s1, s2 = r.s2;
+  const float cc = r.cc, ss = r.ss, c = r.c, s = r.s, ms = -r.s;
   float V00, V01, V10, V11;
   if (s1 < s2) {
     const float tmp = s1; s1 = s2; s2 = tmp;
@@ -193,45 +206,58 @@ __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMateria
   float mass = I.p_mass;
   if (mt == 2) mass = rmul(mass, pdens);
 
-  float4 U, V;
-  float2 sig;
-  jf_svd2(F, U, sig, V);
-  sig.x = fmaxf(sig.x, 1e-6f);
-  sig.y = fmaxf(sig.y, 1e-6f);
-  if (mt == 2) {
-    const float n0 = fminf(fmaxf(sig.x, 0.995f), 1.005f);
-    const float n1 = fminf(fmaxf(sig.y, 0.995f), 1.005f);
-    Jp = rmul(Jp, sig.x / n0);
-    Jp = rmul(Jp, sig.y / n1);
-    sig = make_float2(n0, n1);
-  }
-  const float J = rmul(sig.x, sig.y);
+  const JfSvdRot rot = jf_svd2_values(F);
+  float s00, s01, s10, s11;
   if (mt == 0) {
+    // water: mu = 0, so the corotated term 2 mu (F - R) F^T of the stress is
+    // exactly zero for finite F and only J = s1 s2 is needed (the product
+    // does not depend on the singular values' order); F = sqrt(J) I
+    const float J = rmul(fmaxf(rot.s1, 1e-6f), fmaxf(rot.s2, 1e-6f));
     const float sj = sqrtf(J);
     F = make_float4(sj, 0.0f, 0.0f, sj);
-  } else if (mt == 2) {
-    const float US00 = rmul(U.x, sig.x), US01 = rmul(U.y, sig.y);
-    const float US10 = rmul(U.z, sig.x), US11 = rmul(U.w, sig.y);
-    F = make_float4(rdot2(US00, V.x, US01, V.y), rdot2(US00, V.z, US01, V.w),
-                    rdot2(US10, V.x, US11, V.y), rdot2(US10, V.z, US11, V.w));
-  }
-  const float R00 = rdot2(U.x, V.x, U.y, V.y);
-  const float R01 = rdot2(U.x, V.z, U.y, V.w);
-  const float R10 = rdot2(U.z, V.x, U.w, V.y);
-  const float R11 = rdot2(U.z, V.z, U.w, V.w);
-  const float twomu = rmul(2.0f, mu);
-  const float E00 = rmul(twomu, rsub(F.x, R00)), E01 = rmul(twomu, rsub(F.y, R01));
-  const float E10 = rmul(twomu, rsub(F.z, R10)), E11 = rmul(twomu, rsub(F.w, R11));
-  const float diag = rmul(rmul(la, J), rsub(J, 1.0f));
-  float s00 = radd(rdot2(E00, F.x, E01, F.y), diag);
-  float s01 = rdot2(E00, F.z, E01, F.w);
-  float s10 = rdot2(E10, F.x, E11, F.y);
-  float s11 = radd(rdot2(E10, F.z, E11, F.w), diag);
-  if (mt == 3) {
-    s00 = radd(s00, rmul(rmul(rmul(fiber.x, fiber.x), pressure), J));
-    s01 = radd(s01, rmul(rmul(rmul(fiber.x, fiber.y), pressure), J));
-    s10 = radd(s10, rmul(rmul(rmul(fiber.y, fiber.x), pressure), J));
-    s11 = radd(s11, rmul(rmul(rmul(fiber.y, fiber.y), pressure), J));
+    const float diag = rmul(rmul(la, J), rsub(J, 1.0f));
+    s00 = diag;
+    s01 = 0.0f;
+    s10 = 0.0f;
+    s11 = diag;
+  } else {
+    float4 U, V;
+    float2 sig;
+    jf_svd2_vectors(rot, U, sig, V);
+    sig.x = fmaxf(sig.x, 1e-6f);
+    sig.y = fmaxf(sig.y, 1e-6f);
+    if (mt == 2) {
+      const float n0 = fminf(fmaxf(sig.x, 0.995f), 1.005f);
+      const float n1 = fminf(fmaxf(sig.y, 0.995f), 1.005f);
+      Jp = rmul(Jp, sig.x / n0);
+      Jp = rmul(Jp, sig.y / n1);
+      sig = make_float2(n0, n1);
+    }
+    const float J = rmul(sig.x, sig.y);
+    if (mt == 2) {
+      const float US00 = rmul(U.x, sig.x), US01 = rmul(U.y, sig.y);
+      const float US10 = rmul(U.z, sig.x), US11 = rmul(U.w, sig.y);
+      F = make_float4(rdot2(US00, V.x, US01, V.y), rdot2(US00, V.z, US01, V.w),
+                      rdot2(US10, V.x, US11, V.y), rdot2(US10, V.z, US11, V.w));
+    }
+    const float R00 = rdot2(U.x, V.x, U.y, V.y);
+    const float R01 = rdot2(U.x, V.z, U.y, V.w);
+    const float R10 = rdot2(U.z, V.x, U.w, V.y);
+    const float R11 = rdot2(U.z, V.z, U.w, V.w);
+    const float twomu = rmul(2.0f, mu);
+    const float E00 = rmul(twomu, rsub(F.x, R00)), E01 = rmul(twomu, rsub(F.y, R01));
+    const float E10 = rmul(twomu, rsub(F.z, R10)), E11 = rmul(twomu, rsub(F.w, R11));
+    const float diag = rmul(rmul(la, J), rsub(J, 1.0f));
+    s00 = radd(rdot2(E00, F.x, E01, F.y), diag);
+    s01 = rdot2(E00, F.z, E01, F.w);
+    s10 = rdot2(E10, F.x, E11, F.y);
+    s11 = radd(rdot2(E10, F.z, E11, F.w), diag);
+    if (mt == 3) {
+      s00 = radd(s00, rmul(rmul(rmul(fiber.x, fiber.x), pressure), J));
+      s01 = radd(s01, rmul(rmul(rmul(fiber.x, fiber.y), pressure), J));
+      s10 = radd(s10, rmul(rmul(rmul(fiber.y, fiber.x), pressure), J));
+      s11 = radd(s11, rmul(rmul(rmul(fiber.y, fiber.y), pressure), J));
+    }
   }
   const float k = I.stress_scale;
   o.mass = mass;

@@ -8,7 +8,8 @@
 // The state (x, v, C, F) is checkpointed every K substeps.
 //
 // Backward, per segment in reverse: restore the checkpoint, recompute the
-// segment's K pre-step states, then for each substep in reverse run the
+// segment's K pre-step states and keep each substep's grid (updated
+// velocity, momentum and mass per node), then for each substep in reverse run the
 // hand-written adjoints of G2P (mpm_sim.py:312-333), of the grid update
 // (:274-309) and of P2G (:168-271).  The material map F* -> (F_out, tau)
 // (SVD, plasticity, stress) is differentiated with four-tangent dual numbers
@@ -44,6 +45,7 @@ struct GradArgs {
   const float2* fiber;
   unsigned long long* fix;     // 3 per node: momentum x, momentum y, mass (fixed point)
   float2* u;                   // updated grid velocity
+  float4* pmv;                 // if set: (momentum x, momentum y, mass) per node, kept for the adjoint
   float t;
 };
 
@@ -105,7 +107,9 @@ __global__ void gf_grid(GradArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= I.nx * I.ny) return;
   const unsigned long long* q = a.fix + 3 * (I.g_off + n);
-  a.u[I.g_off + n] = jf_grid_node(I, n % I.nx, n / I.nx, from_fixed(q[0]), from_fixed(q[1]), from_fixed(q[2]));
+  const float px = from_fixed(q[0]), py = from_fixed(q[1]), pm = from_fixed(q[2]);
+  a.u[I.g_off + n] = jf_grid_node(I, n % I.nx, n / I.nx, px, py, pm);
+  if (a.pmv) a.pmv[I.g_off + n] = make_float4(px, py, pm, 0.0f);
 }
 
 __global__ void gf_g2p(GradArgs a) {
@@ -126,7 +130,7 @@ __global__ void gf_g2p(GradArgs a) {
 }
 
 struct AdjArgs {
-  GradArgs f;          // pre-step state of this substep (segment buffer) and recomputed grid
+  GradArgs f;          // pre-step state of this substep (segment buffer) and its kept grid (u, pmv)
   float4* lxv;         // adjoint (x, v): in = post-step, out = pre-step
   float4* lC;
   float4* lF;
@@ -212,8 +216,8 @@ __global__ void ad_grid(AdjArgs A) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= I.nx * I.ny) return;
   const int64_t node = I.g_off + n;
-  const unsigned long long* q = a.fix + 3 * node;
-  const float px = from_fixed(q[0]), py = from_fixed(q[1]), pm = from_fixed(q[2]);
+  const float4 q = a.pmv[node];
+  const float px = q.x, py = q.y, pm = q.z;
   const float2 ub = A.ubar[node];
   if (!(pm > 0.0f)) {
     A.pmbar[node] = make_float4(ub.x, ub.y, 0.0f, 0.0f);
@@ -410,6 +414,8 @@ struct JfGrad {
   float2 *xtmp = nullptr, *vtmp = nullptr;
   float4* ck = nullptr;     // n_ck checkpoints x 3 arrays x total slots
   float4* seg = nullptr;    // K states x 3 arrays x total slots
+  float2* useg = nullptr;   // K grids: updated velocity per node
+  float4* pmseg = nullptr;  // K grids: (momentum x, momentum y, mass) per node
   float4* fin = nullptr;    // final state (3 arrays)
   float* fin_Jp = nullptr;  // final Jp (the backward's recompute updates Jp in place)
   double* gparam = nullptr;
@@ -424,7 +430,7 @@ void jf_grad_free(jf_engine* e) {
   if (!G) return;
   cudaFree(G->fix); cudaFree(G->u); cudaFree(G->ubar); cudaFree(G->pmbar);
   cudaFree(G->lxv); cudaFree(G->lC); cudaFree(G->lF); cudaFree(G->xtmp); cudaFree(G->vtmp);
-  cudaFree(G->ck); cudaFree(G->seg); cudaFree(G->fin); cudaFree(G->fin_Jp); cudaFree(G->gparam);
+  cudaFree(G->ck); cudaFree(G->seg); cudaFree(G->useg); cudaFree(G->pmseg); cudaFree(G->fin); cudaFree(G->fin_Jp); cudaFree(G->gparam);
   cudaFree(G->body_mode); cudaFree(G->inv_n);
   delete G;
   e->grad = nullptr;
@@ -442,6 +448,7 @@ static GradArgs grad_args(jf_engine* e, GradState s, float t) {
   a.fiber = e->p.fiber;
   a.fix = G->fix;
   a.u = G->u;
+  a.pmv = nullptr;
   a.t = t;
   return a;
 }
@@ -459,10 +466,16 @@ static cudaError_t copy_state(jf_engine* e, GradState dst, GradState src) {
   return cudaMemcpyAsync(dst.F, src.F, bytes, cudaMemcpyDeviceToDevice, e->stream);
 }
 
-// one deterministic substep of every instance on state s at time t
-static cudaError_t det_substep(jf_engine* e, GradState s, float t) {
+// one deterministic substep of every instance on state s at time t; with
+// u_keep / pmv_keep set, its grid is written there for the adjoint
+static cudaError_t det_substep(jf_engine* e, GradState s, float t, float2* u_keep = nullptr,
+                               float4* pmv_keep = nullptr) {
   JfGrad* G = e->grad;
-  const GradArgs a = grad_args(e, s, t);
+  GradArgs a = grad_args(e, s, t);
+  if (u_keep) {
+    a.u = u_keep;
+    a.pmv = pmv_keep;
+  }
   cudaError_t err = cudaMemsetAsync(G->fix, 0, sizeof(unsigned long long) * 3 * (size_t)e->total_nodes, e->stream);
   if (err != cudaSuccess) return err;
   const dim3 gp((e->max_slots + kT - 1) / kT, e->M), gn((e->max_cells + kT - 1) / kT, e->M);
@@ -504,8 +517,15 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
   }
   if (G->seg_cap < (size_t)K) {
     cudaFree(G->seg);
+    cudaFree(G->useg);
+    cudaFree(G->pmseg);
     G->seg = nullptr;
+    G->useg = nullptr;
+    G->pmseg = nullptr;
+    G->seg_cap = 0;
     if ((err = alloc_n(&G->seg, 3 * slots * (size_t)K)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->useg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->pmseg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
     G->seg_cap = (size_t)K;
   }
   if ((err = cudaMemcpyAsync(G->body_mode, body_mode, sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream)))
@@ -556,10 +576,12 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
     const int64_t s0 = seg * K;
     const int n = (int)((steps - s0) < K ? (steps - s0) : K);
     if ((err = copy_state(e, work, state_at(G->ck, slots, (size_t)seg))) != cudaSuccess) return err;
+    const size_t nodes = (size_t)e->total_nodes;
     for (int j = 0; j < n; ++j) {
       if ((err = copy_state(e, state_at(G->seg, slots, (size_t)j), work)) != cudaSuccess) return err;
       JfTimed timed(e, true);
-      if ((err = det_substep(e, work, ts[s0 + j])) != cudaSuccess) return err;
+      if ((err = det_substep(e, work, ts[s0 + j], G->useg + nodes * j, G->pmseg + nodes * j)) != cudaSuccess)
+        return err;
     }
     for (int j = n - 1; j >= 0; --j) {
       JfTimed timed(e, false);
@@ -573,20 +595,14 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
       A.xtmp = G->xtmp;
       A.vtmp = G->vtmp;
       A.gparam = G->gparam;
-      // recompute the substep's grid from its pre-step state
-      if ((err = cudaMemsetAsync(G->fix, 0, sizeof(unsigned long long) * 3 * (size_t)e->total_nodes, e->stream)))
-        return err;
-      GradArgs rf = A.f;
-      // P2G writes F/Jp of the state it reads: recompute into the work copy of this pre-step state
-      if ((err = copy_state(e, work, A.f.s)) != cudaSuccess) return err;
-      rf.s = work;
-      gf_p2g<<<gp, kT, 0, e->stream>>>(rf);
-      gf_grid<<<gn, kT, 0, e->stream>>>(rf);
-      if ((err = cudaMemsetAsync(G->ubar, 0, sizeof(float2) * (size_t)e->total_nodes, e->stream))) return err;
+      // the substep's grid as the recompute left it
+      A.f.u = G->useg + nodes * j;
+      A.f.pmv = G->pmseg + nodes * j;
+      if ((err = cudaMemsetAsync(G->ubar, 0, sizeof(float2) * nodes, e->stream))) return err;
       ad_g2p<<<gp, kT, 0, e->stream>>>(A);
       ad_grid<<<gn, kT, 0, e->stream>>>(A);
       ad_p2g<<<gp, kT, 0, e->stream>>>(A);
-      e->launches += 5;
+      e->launches += 3;
       if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
   }

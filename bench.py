@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--grad-only", action="store_true",
+                    help="run only the differentiable leg (8 of the workload's instances) and print it")
     return ap.parse_args()
 
 
@@ -236,7 +238,7 @@ def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
     e.set_stream(stream)
     load_all(e, inputs)
     e.time = 0.0
-    e.grad_forward(10, 10)  # warm-up: buffers, module load
+    e.grad_forward(steps, checkpoint_every)  # warm-up: module load, checkpoint and segment buffers
     e.grad_backward()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     load_all(e, inputs)
@@ -480,10 +482,21 @@ def run_ours(args):
     return 0
 
 
+def run_grad_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    inputs = make_inputs(args.instances, args.slots, 1000)
+    stream = torch.cuda.Stream()
+    print(json.dumps({"differentiable": grad_leg(inputs[:8], 0, stream)}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.grad_only:
+        return run_grad_only(args)
     return run_ours(args)
 
 

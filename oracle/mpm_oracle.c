@@ -14,6 +14,8 @@
  *       grid update             mpm_sim.py:274-309
  *       G2P                     mpm_sim.py:312-333
  *       glow                    mpm_sim.py:336-338
+ *       axisymmetric variant    mpm_sim.py:17,163-165,235-268,292-303
+ *                               (JELLY_AXISYM=1; r_ref set at load, :727)
  *   - payload / body CoM sums   mpm_sim.py:746-762
  * and the third-party 2x2 SVD the reference calls (ti.svd, mpm_sim.py:206):
  * taichi==1.7.4 (uv.lock:1591-1592), python/taichi/_funcs.py _polar_decompose2d
@@ -33,10 +35,12 @@
  *
  * Layouts follow the reference fields (row-major 2x2 matrices):
  *   x, v, fiber: [n][2]   C, F: [n][4] = (00, 01, 10, 11)   material: int32[n]
+ *   r_ref: [n] (load radius, read only in the axisymmetric variant)
  *   grid_v: [nx][ny][2]   grid_m: [nx][ny]      (mpm_sim.py:92-93)
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #ifndef REAL
@@ -60,6 +64,7 @@ typedef struct {
   double contraction;  /* instance_act_contraction[m] mpm_sim.py:121,148 */
   double freq;         /* instance_freq[m]           mpm_sim.py:125,149 */
   double payload_density; /* instance_payload_density[m] mpm_sim.py:142,147 */
+  int32_t axisym;      /* JELLY_AXISYM            mpm_sim.py:17 */
 } oracle_inst;
 
 /* Material constants, Python doubles (mpm_sim.py:25-48). */
@@ -138,7 +143,7 @@ REAL FN(oracle_activation)(const oracle_inst* I, REAL t) {
  * before the step; the caller advances it by (REAL)dt afterwards (:340). */
 void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL* C,
                         REAL* F, const int32_t* mat, REAL* Jp, REAL* glow,
-                        const REAL* fiber, REAL* gv, REAL* gm, REAL t) {
+                        const REAL* fiber, const REAL* r_ref, REAL* gv, REAL* gm, REAL t) {
   const int nx = I->nx, ny = I->ny;
   const double dx_d = 1.0 / nx;
   const double inv_dx_d = (double)nx;
@@ -163,9 +168,18 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
   const REAL act = (REAL)I->actuation;
   const REAL pdens = (REAL)I->payload_density;
 
-  /* 1. grid clear (:160-162) */
+  const int axisym = I->axisym != 0;
+  const REAL rref_lo = (REAL)(dx_d * 0.1), r_lo = (REAL)(dx_d * 0.05);
+
+  /* 1. grid clear (:160-165); the axisymmetric stress sums are scratch here */
   memset(gv, 0, sizeof(REAL) * 2 * (size_t)nx * ny);
   memset(gm, 0, sizeof(REAL) * (size_t)nx * ny);
+  REAL* gsr = NULL;
+  REAL* gsh = NULL;
+  if (axisym) {
+    gsr = (REAL*)calloc((size_t)nx * ny, sizeof(REAL));
+    gsh = (REAL*)calloc((size_t)nx * ny, sizeof(REAL));
+  }
 
   const REAL activation = FN(oracle_activation)(I, t);
 
@@ -254,12 +268,26 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
       s10 = s10 + f1 * f0 * cp * J;
       s11 = s11 + f1 * f1 * cp * J;
     }
+    /* axisymmetric hoop terms, before the scaling (:235-248) */
+    REAL kirch_rr = (REAL)0, kirch_hoop = (REAL)0, r_p = (REAL)0;
+    if (axisym) {
+      kirch_rr = s00;
+      r_p = xp[0];
+      REAL r_ref_p = r_ref[p] > rref_lo ? r_ref[p] : rref_lo;
+      REAL lam = (r_p > r_lo ? r_p : r_lo) / r_ref_p;
+      kirch_hoop = (REAL)2.0 * mu * (lam - (REAL)1.0) + la * J * (J - (REAL)1.0);
+    }
     s00 = stress_scale * s00; s01 = stress_scale * s01;
     s10 = stress_scale * s10; s11 = stress_scale * s11;
     /* APIC affine (:254) */
     REAL af00 = s00 + mass * Cp[0], af01 = s01 + mass * Cp[1];
     REAL af10 = s10 + mass * Cp[2], af11 = s11 + mass * Cp[3];
     REAL mv0 = mass * vp[0], mv1 = mass * vp[1];
+    if (axisym) {  /* ring momentum (mass r_p) v (:264) */
+      REAL mr = mass * r_p;
+      mv0 = mr * vp[0];
+      mv1 = mr * vp[1];
+    }
 
     /* scatter (:256-271) */
     for (int i = 0; i < 3; ++i) {
@@ -272,7 +300,14 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
         size_t node = (size_t)(bx + i) * ny + (size_t)(by + j);
         gv[2 * node] = gv[2 * node] + c0;
         gv[2 * node + 1] = gv[2 * node + 1] + c1;
-        gm[node] = gm[node] + weight * mass;
+        if (axisym) {  /* :264-268 */
+          REAL wm = weight * mass;
+          gm[node] = gm[node] + wm * r_p;
+          gsr[node] = gsr[node] + wm * kirch_rr;
+          gsh[node] = gsh[node] + wm * kirch_hoop;
+        } else {
+          gm[node] = gm[node] + weight * mass;
+        }
       }
     }
   }
@@ -291,7 +326,17 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
       if (j < dcy) damp = damp * ((REAL)0.95 + (REAL)0.05 * (REAL)j / (REAL)dcy);
       if (j > ny - dcy) damp = damp * ((REAL)0.95 + (REAL)0.05 * (REAL)(ny - j) / (REAL)dcy);
       g0 = g0 * damp; g1 = g1 * damp;
-      if (i < 3 && g0 < (REAL)0) g0 = (REAL)0;
+      if (axisym) {
+        /* hoop correction (:295-299), then the axis condition (:302-304) */
+        REAL r_node = ((REAL)i + (REAL)0.5) * dx;
+        if (r_node > dx) {
+          REAL hoop_diff = (gsr[node] - gsh[node]) / m;
+          g0 = g0 + dt * hoop_diff / r_node;
+        }
+        if (i == 0) g0 = (REAL)0;
+      } else if (i < 3 && g0 < (REAL)0) {
+        g0 = (REAL)0;
+      }
       if (i > nx - 3 && g0 > (REAL)0) g0 = (REAL)0;
       if (j < 3 && g1 < (REAL)0) g1 = (REAL)0;
       if (j > ny - 3 && g1 > (REAL)0) g1 = (REAL)0;
@@ -343,6 +388,9 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
     xp[1] = q1 > x_lo ? q1 : x_lo;
   }
 
+  free(gsr);
+  free(gsh);
+
   /* 5. glow (:336-338), every slot */
   for (int64_t p = 0; p < n; ++p) {
     REAL g = glow[p] * (REAL)0.9;
@@ -355,10 +403,10 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
  * like sim_time[None] += dt, mpm_sim.py:340). */
 void FN(oracle_run)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL* C, REAL* F,
                     const int32_t* mat, REAL* Jp, REAL* glow, const REAL* fiber,
-                    REAL* gv, REAL* gm, REAL* t, int64_t steps) {
+                    const REAL* r_ref, REAL* gv, REAL* gm, REAL* t, int64_t steps) {
   const REAL dt = (REAL)I->dt;
   for (int64_t s = 0; s < steps; ++s) {
-    FN(oracle_substep)(I, n, x, v, C, F, mat, Jp, glow, fiber, gv, gm, *t);
+    FN(oracle_substep)(I, n, x, v, C, F, mat, Jp, glow, fiber, r_ref, gv, gm, *t);
     *t = *t + dt;
   }
 }
@@ -370,14 +418,15 @@ void FN(oracle_run)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL* C, 
 void FN(oracle_run_batch)(int32_t M, const oracle_inst* insts, const int64_t* counts,
                           const int64_t* offsets, const int64_t* goffsets, REAL* x, REAL* v,
                           REAL* C, REAL* F, const int32_t* mat, REAL* Jp, REAL* glow,
-                          const REAL* fiber, REAL* gv, REAL* gm, REAL* t, int64_t steps) {
+                          const REAL* fiber, const REAL* r_ref, REAL* gv, REAL* gm, REAL* t,
+                          int64_t steps) {
   const REAL t0 = *t;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int32_t m = 0; m < M; ++m) {
     REAL tm = t0;
     const int64_t o = offsets[m], g = goffsets[m];
     FN(oracle_run)(&insts[m], counts[m], x + 2 * o, v + 2 * o, C + 4 * o, F + 4 * o, mat + o,
-                   Jp + o, glow + o, fiber + 2 * o, gv + 2 * g, gm + g, &tm, steps);
+                   Jp + o, glow + o, fiber + 2 * o, r_ref + o, gv + 2 * g, gm + g, &tm, steps);
   }
   REAL tt = t0;
   const REAL dt = M > 0 ? (REAL)insts[0].dt : (REAL)0;

@@ -6,7 +6,8 @@ never by the product path.
 
 State dictionaries use the reference's field layouts (mpm_sim.py:86-93):
 ``x, v, fiber`` (N,2), ``C, F`` (N,2,2), ``material`` (N,) int32, ``Jp``,
-``glow`` (N,), ``grid_v`` (nx,ny,2), ``grid_m`` (nx,ny).
+``glow`` (N,), ``r_ref`` (N,) (the load radius, mpm_sim.py:727; read only by the
+axisymmetric variant), ``grid_v`` (nx,ny,2), ``grid_m`` (nx,ny).
 """
 from __future__ import annotations
 
@@ -28,7 +29,7 @@ class OracleInst(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("domain_h", ctypes.c_double),
                 ("dt", ctypes.c_double), ("actuation", ctypes.c_double),
                 ("contraction", ctypes.c_double), ("freq", ctypes.c_double),
-                ("payload_density", ctypes.c_double)]
+                ("payload_density", ctypes.c_double), ("axisym", ctypes.c_int32)]
 
 
 @dataclass
@@ -42,10 +43,11 @@ class Instance:
     contraction: float = 0.20       # mpm_sim.py:56,148
     freq: float = 1.0               # mpm_sim.py:149
     payload_density: float = 2.5    # mpm_sim.py:147
+    axisym: bool = False            # JELLY_AXISYM, mpm_sim.py:17
 
     def c(self) -> OracleInst:
         return OracleInst(self.nx, self.ny, self.domain_h, self.dt, self.actuation,
-                          self.contraction, self.freq, self.payload_density)
+                          self.contraction, self.freq, self.payload_density, 1 if self.axisym else 0)
 
 
 def build(force: bool = False) -> str:
@@ -64,12 +66,12 @@ def lib():
         P = ctypes.c_void_p
         for sfx in ("f32", "f64"):
             getattr(L, f"oracle_substep_{sfx}").argtypes = [
-                ctypes.POINTER(OracleInst), ctypes.c_int64] + [P] * 10 + [
+                ctypes.POINTER(OracleInst), ctypes.c_int64] + [P] * 11 + [
                 ctypes.c_float if sfx == "f32" else ctypes.c_double]
             getattr(L, f"oracle_run_{sfx}").argtypes = [
-                ctypes.POINTER(OracleInst), ctypes.c_int64] + [P] * 10 + [P, ctypes.c_int64]
+                ctypes.POINTER(OracleInst), ctypes.c_int64] + [P] * 11 + [P, ctypes.c_int64]
             getattr(L, f"oracle_run_batch_{sfx}").argtypes = [
-                ctypes.c_int32, P, P, P, P] + [P] * 10 + [P, ctypes.c_int64]
+                ctypes.c_int32, P, P, P, P] + [P] * 11 + [P, ctypes.c_int64]
             getattr(L, f"oracle_stats_{sfx}").argtypes = [ctypes.c_int64, P, P, ctypes.c_int32, P]
             getattr(L, f"oracle_svd2_{sfx}").argtypes = [P, P, P, P]
             getattr(L, f"oracle_activation_{sfx}").argtypes = [
@@ -103,6 +105,7 @@ def new_state(pos, mat, fiber=None, precision="f32", nx=128, ny=128):
         "Jp": np.ones(n, dt),
         "glow": np.zeros(n, dt),
         "fiber": np.ascontiguousarray(fiber, dtype=dt).copy(),
+        "r_ref": np.ascontiguousarray(np.asarray(pos)[:, 0], dtype=dt).copy(),
         "grid_v": np.zeros((nx, ny, 2), dt),
         "grid_m": np.zeros((nx, ny), dt),
     }
@@ -118,12 +121,12 @@ def cast_state(state, precision):
 
 def _ptrs(s):
     return [s[k].ctypes.data for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber",
-                                        "grid_v", "grid_m")]
+                                        "r_ref", "grid_v", "grid_m")]
 
 
 def _check(inst: Instance, s):
     dt = s["x"].dtype
-    for k in ("x", "v", "C", "F", "Jp", "glow", "fiber", "grid_v", "grid_m"):
+    for k in ("x", "v", "C", "F", "Jp", "glow", "fiber", "r_ref", "grid_v", "grid_m"):
         assert s[k].dtype == dt and s[k].flags.c_contiguous, k
     assert s["material"].dtype == np.int32 and s["material"].flags.c_contiguous
     assert s["grid_m"].shape == (inst.nx, inst.ny)
@@ -163,7 +166,7 @@ def run_batch(insts, states, t, steps, precision="f32"):
     nodes = np.array([i.nx * i.ny for i in insts], np.int64)
     goffs = np.concatenate([[0], np.cumsum(nodes)[:-1]]).astype(np.int64)
     packed = {}
-    for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber"):
+    for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber", "r_ref"):
         packed[k] = np.ascontiguousarray(np.concatenate([s[k] for s in states], axis=0))
     for k in ("grid_v", "grid_m"):
         packed[k] = np.ascontiguousarray(np.concatenate([s[k].reshape(-1) for s in states]))

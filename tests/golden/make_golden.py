@@ -34,6 +34,10 @@ CASES = {
     "tall_1inst": {"JELLY_INSTANCES": "1", "JELLY_PARTICLES": "1536", "JELLY_GRID_Y": "256",
                    "JELLY_DOMAIN_H": "2.0"},
     "headless_3inst": {"JELLY_INSTANCES": "3", "JELLY_PARTICLES": "2560"},
+    # axisymmetric (r, z) substep, JELLY_AXISYM=1 (mpm_sim.py:17,163-165,235-268,292-303)
+    "axisym_1inst": {"JELLY_INSTANCES": "1", "JELLY_PARTICLES": "3072", "JELLY_AXISYM": "1"},
+    "axisym_tall_2inst": {"JELLY_INSTANCES": "2", "JELLY_PARTICLES": "1536", "JELLY_GRID_Y": "256",
+                          "JELLY_DOMAIN_H": "2.0", "JELLY_AXISYM": "1"},
 }
 
 
@@ -91,9 +95,72 @@ def _perturb(pos, mat, rng, inverted_frac=0.02, vel=0.05):
     return v, C, F, Jp, glow
 
 
+def _axisym_instance(n, rng, y_hi):
+    """Particles crowded near the axis (0.01 < r < 0.06) plus a uniform spread;
+    the load positions set r_ref (mpm_sim.py:727) and the positions written
+    after the load differ radially, so the hoop stretch r / r_ref is not 1.
+    The reference's axisymmetric P2G divides the unweighted stress force by
+    the r-weighted mass, which scales stress near the axis by ~1/r (a 1e-3
+    deformation of payload at r = 0.01 already gives |v| ~ 100 after one
+    substep), so particles at r < 0.2 start stress-free (F = I, C = 0, no
+    muscle) and the deformation, inverted and rotated F, muscle and radial
+    moves (hoop stretch) stay at r > 0.2.  A few stress-free water particles
+    have load radii below the dx/10 floor or positions below dx/20."""
+    pos = np.empty((n, 2), np.float32)
+    near = rng.random(n) < 0.4
+    pos[:, 0] = np.where(near, rng.uniform(0.01, 0.06, n), rng.uniform(0.001, 0.999, n))
+    pos[:, 1] = rng.uniform(0.001, y_hi, n)
+    strip = rng.random(n) < 0.03
+    pos[strip, 0] = rng.uniform(126.0 / 128, 0.999, strip.sum())
+    mat = rng.choice([0, 0, 0, 1, 2, 3, 4], n).astype(np.int32)
+    far = pos[:, 0] > 0.2
+    mat[~far & (mat == 3)] = 1
+    x_now = pos.copy()
+    x_now[far, 0] = np.clip(pos[far, 0] * rng.uniform(0.95, 1.05, far.sum()), 0.001, 0.999)
+    v = rng.normal(0, 0.05, (n, 2)).astype(np.float32)
+    C = rng.normal(0, 0.05, (n, 2, 2)).astype(np.float32)
+    F = (np.eye(2) + rng.normal(0, 0.001, (n, 2, 2))).astype(np.float32)
+    F[(mat == 0) | ~far] = np.eye(2, dtype=np.float32)
+    C[~far] = 0
+    inv = far & (rng.random(n) < 0.03)
+    F[inv, 1, :] *= -1
+    rot = far & (rng.random(n) < 0.05)
+    th = rng.uniform(-0.5, 0.5, rot.sum())
+    R = np.stack([np.stack([np.cos(th), -np.sin(th)], -1), np.stack([np.sin(th), np.cos(th)], -1)], -2)
+    F[rot] = (R @ F[rot].astype(np.float64)).astype(np.float32)
+    edge = rng.random(n) < 0.04
+    tiny_ref = edge & (rng.random(n) < 0.5)
+    tiny_x = edge & ~tiny_ref
+    pos[tiny_ref, 0] = rng.uniform(0.0001, 0.0007, tiny_ref.sum())
+    x_now[tiny_ref, 0] = rng.uniform(0.003, 0.01, tiny_ref.sum())
+    x_now[tiny_x, 0] = rng.uniform(0.0001, 0.0003, tiny_x.sum())
+    mat[edge] = 0
+    F[edge] = np.eye(2, dtype=np.float32)
+    C[edge] = 0
+    dead = rng.random(n) < 0.03
+    mat[dead] = -1
+    pos[dead] = -1
+    x_now[dead] = -1
+    v[dead] = 0
+    C[dead] = 0
+    F[dead] = np.eye(2, dtype=np.float32)
+    Jp = rng.uniform(0.9, 1.1, n).astype(np.float32)
+    glow = rng.uniform(0.0, 0.2, n).astype(np.float32)
+    fib = rng.normal(size=(n, 2)).astype(np.float32)
+    fib /= np.linalg.norm(fib, axis=1, keepdims=True)
+    return dict(pos=pos, x_now=x_now.astype(np.float32), mat=mat, fib=fib, v=v, C=C, F=F, Jp=Jp, glow=glow)
+
+
 def _inputs(case, rng):
     sys.path.insert(0, REPO)
     from jellyfih_b200 import tank
+    if case == "axisym_1inst":
+        params = dict(actuation=[900.0], contraction=[0.4], freq=[1.3], payload_density=[2.5])
+        return [_axisym_instance(3072, rng, 0.999)], params, 0.21, [1, 2]
+    if case == "axisym_tall_2inst":
+        params = dict(actuation=[500.0, 1100.0], contraction=[0.25, 0.5], freq=[1.0, 0.7],
+                      payload_density=[2.5, 3.5])
+        return [_axisym_instance(1536, rng, 1.999) for _ in range(2)], params, 0.03, [1, 2]
     if case == "perturbed_1inst":
         genome = np.concatenate([tank.AURELIA_GENOME, [0.2, 1.0]])
         pos, mat, fib = _robot_window(genome, 4608, (0.40, 0.60, 0.33, 0.47), rng)
@@ -176,12 +243,18 @@ def _run_case(case, reference):
     insts, params, t0, checkpoints = _inputs(case, rng)
     out = {"t0": np.float32(t0), "checkpoints": np.array(checkpoints, np.int32),
            "n_grid": np.int32(sim.n_grid), "n_grid_y": np.int32(sim.n_grid_y),
-           "domain_height": np.float64(sim.domain_height), "dt": np.float64(sim.dt)}
+           "domain_height": np.float64(sim.domain_height), "dt": np.float64(sim.dt),
+           "axisym": np.int32(1 if sim.axisym else 0)}
     for k, vals in params.items():
         out[f"param_{k}"] = np.array(vals, np.float32)
     for m, d in enumerate(insts):
         sim.load_particles(m, d["pos"], d["mat"], d["fib"])
         out[f"in{m}_x"] = d["pos"]
+        if "x_now" in d:
+            # positions moved after the load: r_ref keeps the load radius
+            sim.x.data[m] = d["x_now"]
+            out[f"in{m}_x_load"] = d["pos"]
+            out[f"in{m}_x"] = d["x_now"]
         out[f"in{m}_material"] = d["mat"]
         out[f"in{m}_fiber"] = d["fib"]
         if "v" in d:

@@ -4,11 +4,22 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-STEP_CASES = ("perturbed_1inst", "walls_2inst", "tall_1inst")
+STEP_CASES = ("perturbed_1inst", "walls_2inst", "tall_1inst", "axisym_1inst", "axisym_tall_2inst")
 
 
 def load(case):
     return dict(np.load(os.path.join(GOLDEN, f"{case}.npz")))
+
+
+def axisym(d):
+    """True for fixtures recorded with JELLY_AXISYM=1."""
+    return bool(int(d.get("axisym", 0)))
+
+
+def load_positions(d, m):
+    """Positions given to load_particles (they set r_ref); ``in{m}_x`` holds the
+    positions the substeps start from, written after the load."""
+    return d.get(f"in{m}_x_load", d[f"in{m}_x"])
 
 
 def n_instances(d):

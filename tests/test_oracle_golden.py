@@ -13,16 +13,16 @@ FIELDS = ("x", "v", "C", "F", "Jp", "glow")
 
 
 def _oracle_state(O, d, m):
-    s = O.new_state(d[f"in{m}_x"], d[f"in{m}_material"], d[f"in{m}_fiber"], "f32",
+    s = O.new_state(G.load_positions(d, m), d[f"in{m}_material"], d[f"in{m}_fiber"], "f32",
                     int(d["n_grid"]), int(d["n_grid_y"]))
-    for k in ("v", "C", "F", "Jp", "glow"):
+    for k in ("x", "v", "C", "F", "Jp", "glow"):
         s[k][...] = d[f"in{m}_{k}"]
     return s
 
 
 def _inst(O, d, m):
     return O.Instance(nx=int(d["n_grid"]), ny=int(d["n_grid_y"]), domain_h=float(d["domain_height"]),
-                      dt=float(d["dt"]), **G.instance_params(d, m))
+                      dt=float(d["dt"]), axisym=G.axisym(d), **G.instance_params(d, m))
 
 
 @pytest.mark.parametrize("case", G.STEP_CASES)

@@ -34,6 +34,9 @@ extern "C" {
 
 #define JF_FLAG_GLOW 1u       /* keep the render-only visual_glow field up to date */
 #define JF_FLAG_NO_GRAPHS 2u  /* batched: launch every chunk directly instead of replaying a CUDA graph */
+#define JF_FLAG_AXISYM 4u     /* axisymmetric (r, z) substep, JELLY_AXISYM=1 (mpm_sim.py:17,163-165,
+                                 235-268,292-303): r-weighted P2G, hoop-stress correction, v_r = 0
+                                 on the axis; the differentiable rollout does not support it */
 
 typedef struct jf_engine jf_engine;
 

@@ -20,6 +20,7 @@ JF_PATH_PLAIN = 0
 JF_PATH_BATCHED = 1
 JF_FLAG_GLOW = 1
 JF_FLAG_NO_GRAPHS = 2
+JF_FLAG_AXISYM = 4
 
 
 class JfInstanceDesc(ctypes.Structure):

@@ -61,6 +61,7 @@ struct ChunkArgs {
   float* Jp;
   const float2* fiber;
   float* glow;
+  const float* rref;          // load radius (axisymmetric variant)
   const int32_t* cell_start;  // M x stride: start of each bin's run (relative to p_off)
   const int32_t* cap;         // M: particles a cell lane takes; the rest are overflow
   const int32_t* ovlist;      // overflow positions (relative to p_off), grouped by band
@@ -78,10 +79,11 @@ struct ChunkArgs {
 };
 
 // Shared-memory window of one CTA: grid rows [win0, win0 + WR) of its
-// instance, planar (updated velocity Gx, Gy; accumulated momentum Ax, Ay and
-// mass Am).  Rows outside the window are reached in the owner CTA's window.
+// instance, planar (updated velocity Gx, Gy; accumulated momentum Ax, Ay,
+// mass Am and, axisymmetric only, the hoop sum Ah).  Rows outside the window
+// are reached in the owner CTA's window.
 struct Window {
-  float *Gx, *Gy, *Ax, *Ay, *Am;
+  float *Gx, *Gy, *Ax, *Ay, *Am, *Ah;
   int nx, H, win0, WR;
 };
 
@@ -107,13 +109,14 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
   for (int j = 0; j < 3; ++j) {
     const int row = st.by + j;
     const int wr = row - w.win0;
-    float *px = w.Ax, *py = w.Ay, *pm = w.Am;
+    float *px = w.Ax, *py = w.Ay, *pm = w.Am, *ph = w.Ah;
     int rn = wr * w.nx;
     if (!(wr >= 0 && wr < w.WR)) {
       const int o = owner_of(w, row);
       px = cl.map_shared_rank(w.Ax, o);
       py = cl.map_shared_rank(w.Ay, o);
       pm = cl.map_shared_rank(w.Am, o);
+      if (I.axisym) ph = cl.map_shared_rank(w.Ah, o);
       rn = owner_row(w, row, o) * w.nx;
     }
 #pragma unroll
@@ -122,6 +125,7 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
       atomicAdd(px + rn + st.bx + i, c.x);
       atomicAdd(py + rn + st.bx + i, c.y);
       atomicAdd(pm + rn + st.bx + i, c.z);
+      if (I.axisym) atomicAdd(ph + rn + st.bx + i, jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
     }
   }
 }
@@ -230,6 +234,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   w.Ax = w.Gy + WN;
   w.Ay = w.Ax + WN;
   w.Am = w.Ay + WN;
+  w.Ah = w.Am + WN;  // a sixth plane exists only in the axisymmetric variant
+  const int n_planes = I.axisym ? 6 : 5;
   const int cap = a.cap[m];
   const int tid = threadIdx.x, nth = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, n_warps = nth >> 5;
@@ -242,7 +248,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   float4* __restrict__ F_m = a.F + p0;
   const int32_t* __restrict__ mat_m = a.mat + p0;
 
-  for (int n = tid; n < 5 * WN; n += nth) sm[n] = 0.0f;
+  for (int n = tid; n < n_planes * WN; n += nth) sm[n] = 0.0f;
   unsigned n_fast = 0, n_generic = 0, n_gather_generic = 0, n_overflow = 0;
   cluster.sync();
 
@@ -268,7 +274,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         float4 F = a.F[g];
         const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
         JfScatter sc;
-        jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
+        jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
+                        I.axisym ? a.rref[g] : 1.0f);
         a.F[g] = F;
         if (mt == 2) a.Jp[g] = jp;
         scatter_particle(w, cluster, I, st, sc);
@@ -386,7 +393,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           if (jf_stencil(I, x, st)) {
             const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
             JfScatter sc;
-            jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
+            jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
+                            I.axisym ? a.rref[p0 + k] : 1.0f);
             F_m[k] = F;
             if (mt == 2) a.Jp[p0 + k] = jp;
             const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
@@ -395,6 +403,14 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
             n_generic += in_block ? 0u : 1u;
             if (in_block) {
               accumulate_block(acc, I, st, sc, di, dj);
+              if (I.axisym) {  // the hoop sum goes straight to the window (rows in it)
+                const int hb = (st.by - w.win0) * nx + st.bx;
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                  for (int ii = 0; ii < 3; ++ii)
+                    atomicAdd(w.Ah + hb + jj * nx + ii, jf_w(st, 0, ii) * jf_w(st, 1, jj) * sc.hoop);
+              }
             } else {
               scatter_particle(w, cluster, I, st, sc);
             }
@@ -416,7 +432,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         const int j = w.win0 + wr;
         if ((j >= row0 && j < own_hi) || j < 0 || j >= ny) continue;
         const float vx = w.Ax[n], vy = w.Ay[n], vm = w.Am[n];
-        if (vx != 0.0f || vy != 0.0f || vm != 0.0f) {
+        const float vh = I.axisym ? w.Ah[n] : 0.0f;
+        if (vx != 0.0f || vy != 0.0f || vm != 0.0f || vh != 0.0f) {
           const int o = owner_of(w, j);
           const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
           atomicAdd(cluster.map_shared_rank(w.Ax, o) + rn, vx);
@@ -425,6 +442,10 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           w.Ax[n] = 0.0f;
           w.Ay[n] = 0.0f;
           w.Am[n] = 0.0f;
+          if (I.axisym) {
+            atomicAdd(cluster.map_shared_rank(w.Ah, o) + rn, vh);
+            w.Ah[n] = 0.0f;
+          }
         }
       }
       cluster.sync();
@@ -437,13 +458,14 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         const int i = n - wr * nx;
         const int j = w.win0 + wr;
         const float mm = w.Am[n];
-        const float2 u = jf_grid_node(I, i, j, w.Ax[n], w.Ay[n], mm);
+        const float2 u = jf_grid_node(I, i, j, w.Ax[n], w.Ay[n], mm, I.axisym ? w.Ah[n] : 0.0f);
         w.Gx[n] = u.x;
         w.Gy[n] = u.y;
         if (last) a.grid[I.g_off + (int64_t)j * nx + i] = make_float4(u.x, u.y, mm, 0.0f);
         w.Ax[n] = 0.0f;
         w.Ay[n] = 0.0f;
         w.Am[n] = 0.0f;
+        if (I.axisym) w.Ah[n] = 0.0f;
       }
       cluster.sync();
 
@@ -638,6 +660,7 @@ __global__ void sort_scatter_kernel(const JfInst* __restrict__ inst, const int32
   dst.Jp[d] = src.Jp[g];
   dst.glow[d] = src.glow[g];
   dst.slot[d] = src.slot[g];
+  dst.rref[d] = src.rref[g];
 }
 
 // Dead slots are not streamed by the chunk kernel; their render-only glow
@@ -667,7 +690,8 @@ __global__ void advance_time_kernel(float* t, int K, float dt) {
 }  // namespace
 
 size_t jf_batched_smem_bytes(const jf_engine* e) {
-  return sizeof(float) * 5 * (size_t)e->win_nodes;
+  const size_t planes = (e->flags & JF_FLAG_AXISYM) ? 6 : 5;
+  return sizeof(float) * planes * (size_t)e->win_nodes;
 }
 
 cudaError_t jf_batched_sort(jf_engine* e) {
@@ -708,6 +732,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.Jp = e->p.Jp;
   a.fiber = e->p.fiber;
   a.glow = e->p.glow;
+  a.rref = e->p.rref;
   a.cell_start = e->d_counts;
   a.cap = e->d_cap;
   a.ovlist = e->d_ovlist;

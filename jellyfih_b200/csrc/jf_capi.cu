@@ -53,12 +53,13 @@ cudaError_t alloc_particles(JfParticles& p, size_t n) {
   if ((err = alloc(&p.Jp, n)) != cudaSuccess) return err;
   if ((err = alloc(&p.glow, n)) != cudaSuccess) return err;
   if ((err = alloc(&p.slot, n)) != cudaSuccess) return err;
+  if ((err = alloc(&p.rref, n)) != cudaSuccess) return err;
   return cudaSuccess;
 }
 
 void free_particles(JfParticles& p) {
   cudaFree(p.xv); cudaFree(p.C); cudaFree(p.F); cudaFree(p.mat);
-  cudaFree(p.fiber); cudaFree(p.Jp); cudaFree(p.glow); cudaFree(p.slot);
+  cudaFree(p.fiber); cudaFree(p.Jp); cudaFree(p.glow); cudaFree(p.slot); cudaFree(p.rref);
   p = JfParticles();
 }
 
@@ -274,7 +275,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   int64_t p_off = 0, g_off = 0;
   for (int m = 0; m < e->M; ++m) {
     const jf_instance_desc& d = cfg->instances[m];
-    JfInst I;
+    JfInst I = {};
     const double nx = d.n_grid;
     const double dx_d = 1.0 / nx;
     const double p_vol = (dx_d * 0.5) * (dx_d * 0.5);
@@ -294,6 +295,9 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     I.c4 = (float)(4 * nx);
     I.dtg = (float)(e->dt * 10.0);
     I.y_hi = (float)((double)d.domain_height - 0.001);
+    I.rref_lo = (float)(dx_d * 0.1);
+    I.r_lo = (float)(dx_d * 0.05);
+    I.axisym = (cfg->flags & JF_FLAG_AXISYM) ? 1 : 0;
     I.domain_h = (double)d.domain_height;
     e->inst.push_back(I);
     JfParams P = {500.0f, 0.20f, 1.0f, 2.5f};  // mpm_sim.py:143-149
@@ -558,6 +562,8 @@ int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts
 int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss) {
   if (check_engine(e)) return JF_ERR_INVALID;
   if (steps <= 0 || checkpoint_every <= 0) return fail(e, JF_ERR_INVALID, "steps and checkpoint_every must be > 0");
+  if (e->flags & JF_FLAG_AXISYM)
+    return fail(e, JF_ERR_UNSUPPORTED, "the differentiable rollout has no axisymmetric variant");
   int rc = set_device(e);
   if (rc) return rc;
   if ((rc = upload_params(e))) return rc;

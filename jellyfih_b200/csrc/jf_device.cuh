@@ -27,6 +27,9 @@ struct JfInst {
   float c4;             // 4 * inv_dx (:326)
   float dtg;            // dt * gravity (:329)
   float y_hi;           // domain_height - 0.001 (:333)
+  float rref_lo;        // axisymmetric: dx * 0.1, floor of the load radius (:246)
+  float r_lo;           // axisymmetric: dx * 0.05, floor of the radius (:247)
+  int32_t axisym;       // JELLY_AXISYM (:17): r-weighted P2G, hoop correction, axis condition
   double domain_h;      // domain_height as the caller gave it (fitness ceiling, evolve.py:101)
 };
 
@@ -174,11 +177,14 @@ __device__ __forceinline__ float jf_w(const JfStencil& s, int axis, int k) {
   return k == 0 ? s.wy0 : (k == 1 ? s.wy1 : s.wy2);
 }
 
-// Per-particle scatter terms of P2G: mass, APIC affine matrix and momentum.
+// Per-particle scatter terms of P2G: the mass channel (mass, times the radius
+// r_p in the axisymmetric variant), APIC affine matrix, momentum (mass r_p v
+// there) and, axisymmetric only, mass * (sigma_rr - sigma_thetatheta).
 struct JfScatter {
   float mass;
   float af00, af01, af10, af11;
   float mv0, mv1;
+  float hoop;
 };
 
 // P2G for one particle (mpm_sim.py:189-254): F <- (I + dt C) F, SVD,
@@ -186,10 +192,12 @@ struct JfScatter {
 // F = sqrt(J) I), fixed-corotated Kirchhoff stress plus the muscle's active
 // fibre stress, scaled, plus the APIC term.  Jp is updated only when the
 // material is payload (for every other material the ratio is exactly 1).
+// Axisymmetric variant (:235-268): xr = the particle's radius x[0], rref its
+// load radius; the hoop stress uses the stretch max(xr, dx/20) / max(rref, dx/10).
 __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMaterials& mats, int mt,
                                                 float2 v, float4 C, float4& F, float& Jp,
                                                 float2 fiber, float pressure, float pdens,
-                                                JfScatter& o) {
+                                                JfScatter& o, float xr = 0.0f, float rref = 1.0f) {
   const float dt = I.dt;
   {
     const float A00 = radd(1.0f, rmul(dt, C.x)), A01 = rmul(dt, C.y);
@@ -207,12 +215,12 @@ __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMateria
   if (mt == 2) mass = rmul(mass, pdens);
 
   const JfSvdRot rot = jf_svd2_values(F);
-  float s00, s01, s10, s11;
+  float s00, s01, s10, s11, J;
   if (mt == 0) {
     // water: mu = 0, so the corotated term 2 mu (F - R) F^T of the stress is
     // exactly zero for finite F and only J = s1 s2 is needed (the product
     // does not depend on the singular values' order); F = sqrt(J) I
-    const float J = rmul(fmaxf(rot.s1, 1e-6f), fmaxf(rot.s2, 1e-6f));
+    J = rmul(fmaxf(rot.s1, 1e-6f), fmaxf(rot.s2, 1e-6f));
     const float sj = sqrtf(J);
     F = make_float4(sj, 0.0f, 0.0f, sj);
     const float diag = rmul(rmul(la, J), rsub(J, 1.0f));
@@ -233,7 +241,7 @@ __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMateria
       Jp = rmul(Jp, sig.y / n1);
       sig = make_float2(n0, n1);
     }
-    const float J = rmul(sig.x, sig.y);
+    J = rmul(sig.x, sig.y);
     if (mt == 2) {
       const float US00 = rmul(U.x, sig.x), US01 = rmul(U.y, sig.y);
       const float US10 = rmul(U.z, sig.x), US11 = rmul(U.w, sig.y);
@@ -260,13 +268,25 @@ __device__ __forceinline__ void jf_p2g_particle(const JfInst& I, const JfMateria
     }
   }
   const float k = I.stress_scale;
-  o.mass = mass;
+  float mch = mass;
+  o.hoop = 0.0f;
+  if (I.axisym) {
+    // sigma_rr is the unscaled stress s00; for water (mu = 0) sigma_thetatheta
+    // equals it exactly, so its hoop term is zero
+    if (mt != 0) {
+      const float lam = __fdiv_rn(fmaxf(xr, I.r_lo), fmaxf(rref, I.rref_lo));
+      const float khoop = radd(rmul(rmul(2.0f, mu), rsub(lam, 1.0f)), rmul(rmul(la, J), rsub(J, 1.0f)));
+      o.hoop = rmul(mass, rsub(s00, khoop));
+    }
+    mch = rmul(mass, xr);
+  }
+  o.mass = mch;
   o.af00 = rdot2(k, s00, mass, C.x);
   o.af01 = rdot2(k, s01, mass, C.y);
   o.af10 = rdot2(k, s10, mass, C.z);
   o.af11 = rdot2(k, s11, mass, C.w);
-  o.mv0 = rmul(mass, v.x);
-  o.mv1 = rmul(mass, v.y);
+  o.mv0 = rmul(mch, v.x);
+  o.mv1 = rmul(mch, v.y);
 }
 
 // Contribution of a particle to stencil node (i, j), i, j in 0..2
@@ -284,8 +304,11 @@ __device__ __forceinline__ float3 jf_node_contrib(const JfInst& I, const JfStenc
 // Grid node update (mpm_sim.py:274-309): normalise by mass, damp in a band of
 // n//20 nodes on all four sides, zero the velocity component pointing into a
 // wall within 3 nodes.  Nodes without mass keep their (zero) momentum.
+// Axisymmetric variant (:292-303): h = sum of mass * (sigma_rr - sigma_tt);
+// v_r += dt (h / m) / r_node off the axis cell, v_r = 0 on the axis (i = 0)
+// instead of the i < 3 wall.
 __device__ __forceinline__ float2 jf_grid_node(const JfInst& I, int i, int j, float gx, float gy,
-                                               float m) {
+                                               float m, float h = 0.0f) {
   if (!(m > 0.0f)) return make_float2(gx, gy);
   float g0 = gx / m, g1 = gy / m;
   float damp = 1.0f;
@@ -295,7 +318,13 @@ __device__ __forceinline__ float2 jf_grid_node(const JfInst& I, int i, int j, fl
   if (j > I.ny - I.dcy) damp = damp * (0.95f + 0.05f * (float)(I.ny - j) / (float)I.dcy);
   g0 = g0 * damp;
   g1 = g1 * damp;
-  if (i < 3 && g0 < 0.0f) g0 = 0.0f;
+  if (I.axisym) {
+    const float r_node = ((float)i + 0.5f) * I.dx;
+    if (r_node > I.dx) g0 = g0 + (I.dt * (h / m)) / r_node;
+    if (i == 0) g0 = 0.0f;
+  } else if (i < 3 && g0 < 0.0f) {
+    g0 = 0.0f;
+  }
   if (i > I.nx - 3 && g0 > 0.0f) g0 = 0.0f;
   if (j < 3 && g1 < 0.0f) g1 = 0.0f;
   if (j > I.ny - 3 && g1 > 0.0f) g1 = 0.0f;

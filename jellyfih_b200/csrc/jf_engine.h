@@ -23,6 +23,7 @@ struct JfParticles {
   float* Jp = nullptr;      // plastic volume ratio
   float* glow = nullptr;    // render-only glow
   int32_t* slot = nullptr;  // engine position -> slot index
+  float* rref = nullptr;    // load radius x[0] (axisymmetric hoop stretch)
 };
 
 struct JfGrad;

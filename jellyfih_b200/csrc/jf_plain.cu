@@ -31,7 +31,7 @@ __global__ void plain_p2g(JfInst I, JfMaterials mats, JfParams P, float pressure
                           const float4* __restrict__ xv, const float4* __restrict__ Cm,
                           float4* __restrict__ Fm, const int32_t* __restrict__ mat,
                           float* __restrict__ Jp, const float2* __restrict__ fiber,
-                          float4* __restrict__ grid) {
+                          const float* __restrict__ rref, float4* __restrict__ grid) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= I.n_slots) return;
   const int64_t g = I.p_off + k;
@@ -46,7 +46,8 @@ __global__ void plain_p2g(JfInst I, JfMaterials mats, JfParams P, float pressure
   float jp = (mt == 2) ? Jp[g] : 1.0f;
   const float2 fb = (mt == 3) ? fiber[g] : make_float2(0.0f, 1.0f);
   JfScatter sc;
-  jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc);
+  jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
+                  I.axisym ? rref[g] : 1.0f);
   Fm[g] = F;
   if (mt == 2) Jp[g] = jp;
   float4* gi = grid + I.g_off;
@@ -55,7 +56,8 @@ __global__ void plain_p2g(JfInst I, JfMaterials mats, JfParams P, float pressure
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       const float3 c = jf_node_contrib(I, st, sc, i, j);
-      atomicAdd(gi + (int64_t)(st.by + j) * I.nx + (st.bx + i), make_float4(c.x, c.y, c.z, 0.0f));
+      const float hw = jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop;  // axisymmetric hoop channel
+      atomicAdd(gi + (int64_t)(st.by + j) * I.nx + (st.bx + i), make_float4(c.x, c.y, c.z, hw));
     }
   }
 }
@@ -65,7 +67,7 @@ __global__ void plain_grid(JfInst I, float4* __restrict__ grid) {
   if (n >= I.nx * I.ny) return;
   const int i = n % I.nx, j = n / I.nx;
   const float4 g = grid[I.g_off + n];
-  const float2 u = jf_grid_node(I, i, j, g.x, g.y, g.z);
+  const float2 u = jf_grid_node(I, i, j, g.x, g.y, g.z, g.w);
   grid[I.g_off + n] = make_float4(u.x, u.y, g.z, 0.0f);
 }
 
@@ -147,6 +149,7 @@ __global__ void load_kernel(JfInst I, int32_t n, const float* __restrict__ pos,
   p.Jp[g] = 1.0f;
   p.glow[g] = glow_slot[k];
   p.slot[g] = k;
+  p.rref[g] = x.x;  // mpm_sim.py:727
 }
 
 __global__ void glow_to_slot_kernel(JfInst I, const float* __restrict__ glow,
@@ -234,7 +237,8 @@ cudaError_t jf_plain_step(jf_engine* e, int64_t n_steps) {
       if (err != cudaSuccess) return err;
       if (I.n_slots > 0) {
         plain_p2g<<<blocks_for(I.n_slots), kThreads, 0, e->stream>>>(
-            I, mats, P, pressure, e->p.xv, e->p.C, e->p.F, e->p.mat, e->p.Jp, e->p.fiber, e->d_grid);
+            I, mats, P, pressure, e->p.xv, e->p.C, e->p.F, e->p.mat, e->p.Jp, e->p.fiber, e->p.rref,
+            e->d_grid);
       }
       plain_grid<<<blocks_for(nodes), kThreads, 0, e->stream>>>(I, e->d_grid);
       if (I.n_slots > 0) {

@@ -43,19 +43,22 @@ class Engine:
     ``path='batched'`` advances every instance in one persistent cluster launch
     per chunk; ``path='plain'`` launches clear / P2G / grid update / G2P per
     instance and substep, as the reference's substep() offloads do.
+    ``axisym=True`` runs the axisymmetric (r, z) substep of JELLY_AXISYM=1
+    (every instance; the load positions' x becomes each particle's r_ref).
     """
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
                  block_threads: int = 512, cluster_size: int = 0, graphs: bool = True,
-                 cell_cap: int = 0):
+                 cell_cap: int = 0, axisym: bool = False):
         self._lib = L.load()
         self.instances = list(instances)
         self.M = len(self.instances)
         self.path = path
         descs = (L.JfInstanceDesc * self.M)(*[
             L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
-        flags = (L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
+        flags = ((L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
+                 | (L.JF_FLAG_AXISYM if axisym else 0))
         cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
                          flags, device, resort_interval, block_threads, cluster_size, cell_cap)
         h = L._E()
@@ -65,7 +68,7 @@ class Engine:
         self._h = h
         self.dt = dt
         self.config = dict(path=path, resort_interval=resort_interval, block_threads=block_threads,
-                           cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap)
+                           cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap, axisym=axisym)
 
     # -- plumbing --------------------------------------------------------
     def _check(self, rc):

@@ -14,8 +14,9 @@ available as ``mpm_sim.ti.sync()``.
 
 Engine selection (not in the reference): JELLY_B200_PATH = batched (default)
 or plain; JELLY_B200_GLOW = 1 keeps the render-only visual_glow updated.
-JELLY_AXISYM=1 is rejected: the axisymmetric variant is not implemented.
-The renderer kernels (mpm_sim.py:343-712) are not provided.
+JELLY_AXISYM=1 selects the axisymmetric (r, z) substep, as in the reference;
+its r_ref (the load radius) lives inside the engine and is not exposed as a
+field.  The renderer kernels (mpm_sim.py:343-712) are not provided.
 """
 from __future__ import annotations
 
@@ -33,9 +34,7 @@ n_particles = int(os.environ.get("JELLY_PARTICLES", "80000"))
 n_grid = 128 * quality
 n_grid_y = int(os.environ.get("JELLY_GRID_Y", str(n_grid)))
 domain_height = float(os.environ.get("JELLY_DOMAIN_H", "1.0"))
-axisym = os.environ.get("JELLY_AXISYM", "0") == "1"
-if axisym:
-    raise NotImplementedError("JELLY_AXISYM=1: the axisymmetric substep is not implemented")
+axisym = os.environ.get("JELLY_AXISYM", "0") == "1"  # axisymmetric (r, z) MPM, mpm_sim.py:17
 dx, inv_dx = 1 / n_grid, float(n_grid)
 dt = 2e-5 / quality
 p_vol = (dx * 0.5) ** 2
@@ -72,10 +71,11 @@ video_res = 1024
 grid_side = int(math.ceil(math.sqrt(n_instances)))
 res_sub = video_res // grid_side
 
-print(f"Allocating {n_instances} instances with {n_particles} particles each...")
+print(f"Allocating {n_instances} instances with {n_particles} particles each..."
+      + (" [AXISYM mode: JELLY_AXISYM=1]" if axisym else ""))
 _engine = Engine([InstanceSpec(n_particles, n_grid, n_grid_y, domain_height)] * n_instances,
                  path=os.environ.get("JELLY_B200_PATH", "batched"), dt=dt,
-                 glow=os.environ.get("JELLY_B200_GLOW", "0") == "1")
+                 glow=os.environ.get("JELLY_B200_GLOW", "0") == "1", axisym=axisym)
 
 
 def engine() -> Engine:
@@ -231,7 +231,7 @@ material = _ParticleField("material")
 Jp = _ParticleField("Jp")
 visual_glow = _ParticleField("glow")
 fiber_dir = _ParticleField("fiber")
-r_ref = None  # axisymmetric-only field (mpm_sim.py:131), not provided
+r_ref = None  # axisymmetric load radius (mpm_sim.py:131): kept inside the engine
 grid_v = _GridField(0)
 grid_m = _GridField(1)
 sim_time = _TimeField()

@@ -15,9 +15,15 @@ default output matches fill_tank):
 * ``spacing_div``: lattice spacing dx / spacing_div (the reference uses 2).
 * ``jitter``: seeded uniform jitter of every live particle by +-jitter*dx.
 
+The axisymmetric mode (make_jelly.py:13-14,275-307: the right half-profile is
+the whole cross-section, payload over r in [0, W/2]) follows the reference's
+JELLY_AXISYM environment variable unless ``axisym`` is passed explicitly.
+
 Gene bounds follow evolve.py:55-62.
 """
 from __future__ import annotations
+
+import os
 
 import numpy as np
 from scipy.spatial import cKDTree
@@ -26,6 +32,12 @@ PAYLOAD_WIDTH = 0.08                       # make_jelly.py:8
 PAYLOAD_HEIGHT = 0.05                      # make_jelly.py:9
 DEFAULT_SPAWN = np.array([0.5, 0.40])      # make_jelly.py:10
 TALL_SPAWN = np.array([0.5, 0.60])         # evolve.py:136
+AXISYM_SPAWN = np.array([0.0, 0.40])       # make_jelly.py:11
+
+
+def _axisym_default(axisym):
+    """make_jelly.py:14 reads JELLY_AXISYM once at import; here per call."""
+    return os.environ.get("JELLY_AXISYM", "0") == "1" if axisym is None else bool(axisym)
 
 # evolve.py:60-61: [cp1_x, cp1_y, cp2_x, cp2_y, end_x, end_y, t_base, t_mid,
 # t_tip, contraction_frac, freq_mult]
@@ -107,7 +119,7 @@ def _normals_2d(points):
     return normals / norm
 
 
-def generate_phenotype(genome, spawn_offset=None, grid_res=128, with_payload=True):
+def generate_phenotype(genome, spawn_offset=None, grid_res=128, with_payload=True, axisym=None):
     """Genome -> (pos (K,2) f64, mat (K,) int, fiber (K,2) f32, self_intersecting).
 
     Follows make_jelly.py:74-334 step by step: Bezier spine from genes 0-5,
@@ -226,7 +238,13 @@ def generate_phenotype(genome, spawn_offset=None, grid_res=128, with_payload=Tru
         _, sp_idx = spine_tree.query(right_points[muscle_mask_r])
         right_fiber[muscle_mask_r] = spine_tangents[sp_idx]
 
-    if len(right_points) > 0:
+    axisym = _axisym_default(axisym)
+    if axisym:
+        # make_jelly.py:276-280: the right half-profile is the whole (r >= 0) section
+        all_soft_pos = right_points
+        all_soft_mats = right_mats
+        all_soft_fiber = right_fiber
+    elif len(right_points) > 0:
         left_pos = right_points.copy()
         left_pos[:, 0] *= -1
         left_fiber = right_fiber.copy()
@@ -241,7 +259,10 @@ def generate_phenotype(genome, spawn_offset=None, grid_res=128, with_payload=Tru
 
     payload_particles = None
     if with_payload:
-        px = np.linspace(-PAYLOAD_WIDTH / 2, PAYLOAD_WIDTH / 2, int(PAYLOAD_WIDTH * raster_res))
+        if axisym:  # make_jelly.py:300-301
+            px = np.linspace(0, PAYLOAD_WIDTH / 2, int(PAYLOAD_WIDTH / 2 * raster_res))
+        else:
+            px = np.linspace(-PAYLOAD_WIDTH / 2, PAYLOAD_WIDTH / 2, int(PAYLOAD_WIDTH * raster_res))
         py = np.linspace(0, PAYLOAD_HEIGHT, int(PAYLOAD_HEIGHT * raster_res))
         pgx, pgy = np.meshgrid(px, py)
         payload_particles = np.vstack([pgx.ravel(), pgy.ravel()]).T
@@ -265,7 +286,8 @@ def generate_phenotype(genome, spawn_offset=None, grid_res=128, with_payload=Tru
 
 
 def fill_tank(genome, max_particles, grid_res=128, spawn_offset=None, water_margin=0.005,
-              with_payload=True, domain_height=1.0, spacing_div=2.0, jitter=0.0, seed=None):
+              with_payload=True, domain_height=1.0, spacing_div=2.0, jitter=0.0, seed=None,
+              axisym=None):
     """Robot + water lattice padded to ``max_particles`` slots (make_jelly.py:336-402).
 
     Returns (positions f32 (N,2), materials i32 (N,), fibers f32 (N,2), stats).
@@ -275,7 +297,7 @@ def fill_tank(genome, max_particles, grid_res=128, spawn_offset=None, water_marg
     if spawn_offset is None:
         spawn_offset = DEFAULT_SPAWN
     robot_pos, robot_mat, robot_fiber, self_intersecting = generate_phenotype(
-        genome, spawn_offset, grid_res=grid_res, with_payload=with_payload)
+        genome, spawn_offset, grid_res=grid_res, with_payload=with_payload, axisym=axisym)
     n_robot = len(robot_pos)
 
     spacing = 1.0 / (grid_res * spacing_div)

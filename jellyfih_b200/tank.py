@@ -90,17 +90,28 @@ def _segments_intersect(a, b, c, d):
 
 
 def polygon_self_intersects(polygon) -> bool:
-    """make_jelly.py:46-58: any non-adjacent edge pair crossing."""
-    n = len(polygon)
-    for i in range(n):
-        a, b = polygon[i], polygon[(i + 1) % n]
-        for j in range(i + 2, n):
-            if j == n - 1 and i == 0:
-                continue
-            c, d = polygon[j], polygon[(j + 1) % n]
-            if _segments_intersect(a, b, c, d):
-                return True
-    return False
+    """make_jelly.py:46-58: any non-adjacent edge pair crossing.
+
+    The pair loop of the reference, evaluated for all pairs at once with the
+    same float64 operations as _segments_intersect (same decisions)."""
+    P = np.asarray(polygon, dtype=np.float64)
+    n = len(P)
+    if n < 4:
+        return False
+    i, j = np.triu_indices(n, k=2)
+    keep = ~((i == 0) & (j == n - 1))
+    i, j = i[keep], j[keep]
+    a, b = P[i], P[(i + 1) % n]
+    c, d = P[j], P[(j + 1) % n]
+    r = b - a
+    s = d - c
+    rxs = r[:, 0] * s[:, 1] - r[:, 1] * s[:, 0]
+    ok = np.abs(rxs) >= 1e-12
+    qp = c - a
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = (qp[:, 0] * s[:, 1] - qp[:, 1] * s[:, 0]) / rxs
+        u = (qp[:, 0] * r[:, 1] - qp[:, 1] * r[:, 0]) / rxs
+    return bool(np.any(ok & (t > 0) & (t < 1) & (u > 0) & (u < 1)))
 
 
 def cubic_bezier(p0, p1, p2, p3, t):
@@ -307,8 +318,11 @@ def fill_tank(genome, max_particles, grid_res=128, spawn_offset=None, water_marg
     wgx, wgy = np.meshgrid(wx, wy)
     water_candidates = np.vstack([wgx.ravel(), wgy.ravel()]).T
     if n_robot > 0:
+        # make_jelly.py:361-364.  The search is bounded just above the margin:
+        # candidates with no robot point that close come back at distance inf,
+        # the others with their exact distance, so the kept set is the same.
         tree = cKDTree(robot_pos)
-        distances, _ = tree.query(water_candidates, k=1)
+        distances, _ = tree.query(water_candidates, k=1, distance_upper_bound=water_margin * (1 + 1e-9))
         water_pos = water_candidates[distances > water_margin]
     else:
         water_pos = water_candidates

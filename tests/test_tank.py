@@ -72,3 +72,36 @@ def test_tall_tank_and_coarse_grid():
     assert 115000 < st["n_total"] <= 160000 and pos[mat >= 0, 1].max() > 1.9
     pos, mat, _, st = tank.fill_tank(g, 24000, grid_res=64)
     assert 14000 < st["n_total"] < 24000
+
+
+def _self_intersects_loop(polygon):
+    """The reference's pair loop (make_jelly.py:46-58) over _segments_intersect."""
+    n = len(polygon)
+    for i in range(n):
+        a, b = polygon[i], polygon[(i + 1) % n]
+        for j in range(i + 2, n):
+            if j == n - 1 and i == 0:
+                continue
+            if tank._segments_intersect(a, b, polygon[j], polygon[(j + 1) % n]):
+                return True
+    return False
+
+
+def test_vectorised_self_intersection_matches_the_pair_loop():
+    rng = np.random.default_rng(11)
+    verdicts = []
+    for k in range(60):
+        n = int(rng.integers(4, 40))
+        if k % 2:
+            # star-shaped polygon ordered by angle: simple (no crossing)
+            th = np.sort(rng.uniform(0, 2 * np.pi, n))
+            poly = np.stack([np.cos(th), np.sin(th)], 1) * rng.uniform(0.5, 1.0, (n, 1))
+        else:
+            poly = rng.uniform(0, 1, (n, 2))
+        got = tank.polygon_self_intersects(poly)
+        assert got == _self_intersects_loop(poly), k
+        verdicts.append(got)
+    assert any(verdicts) and not all(verdicts)
+    for g in tank.uniform_genomes(8, 5):
+        pos, mat, fib, st = tank.fill_tank(g, 80000)
+        assert isinstance(st["self_intersecting"], bool)

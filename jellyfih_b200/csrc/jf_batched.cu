@@ -66,6 +66,7 @@ struct ChunkArgs {
   const int32_t* cap;         // M: particles a cell lane takes; the rest are overflow
   const int32_t* ovlist;      // overflow positions (relative to p_off), grouped by band
   const int32_t* ovband;      // M x (CS + 1): band starts in ovlist
+  const int32_t* order;       // cluster -> instance
   int32_t stride;
   float4* grid;             // grid of the chunk's last substep, node = g_off + j * nx + i
   int32_t* err;
@@ -214,8 +215,9 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   cg::cluster_group cluster = cg::this_cluster();
   const int CS = a.CS;
   const int r = (int)cluster.block_rank();
-  const int m = blockIdx.x / CS;
-  if (m >= a.M) return;  // a padding cluster leaves as a whole
+  const int ci = blockIdx.x / CS;
+  if (ci >= a.M) return;  // a padding cluster leaves as a whole
+  const int m = a.order[ci];
 
   const JfInst I = a.inst[m];
   const JfParams P = a.params[m];
@@ -737,6 +739,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.cap = e->d_cap;
   a.ovlist = e->d_ovlist;
   a.ovband = e->d_ovband;
+  a.order = e->d_order;
   a.stride = e->max_cells + 2;
   a.grid = e->d_grid;
   a.err = e->d_err;

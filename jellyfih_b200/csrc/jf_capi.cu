@@ -342,10 +342,17 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
         (err = alloc(&e->d_counts, (size_t)(e->max_cells + 2) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_cap, e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_order, e->M)) != cudaSuccess ||
         (err = alloc(&e->d_path, 4)) != cudaSuccess ||
         (err = alloc(&e->d_time, 1)) != cudaSuccess ||
         (err = cudaMemset(e->d_path, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
       return bail(JF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+    e->n_live.assign(e->M, 0);
+    e->h_order.resize(e->M);
+    for (int m = 0; m < e->M; ++m) e->h_order[m] = m;
+    if ((err = cudaMemcpy(e->d_order, e->h_order.data(), sizeof(int32_t) * e->M, cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+      return bail(JF_ERR_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(err));
     if ((err = jf_batched_prepare(e)) != cudaSuccess)
       return bail(JF_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(err));
     int active = 0;
@@ -382,7 +389,7 @@ int jf_destroy(jf_engine* e) {
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_rank); cudaFree(e->d_ovlist); cudaFree(e->d_ovband); cudaFree(e->d_ovcur);
-  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
+  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
@@ -436,6 +443,18 @@ int jf_load_instance(jf_engine* e, int32_t m, const float* pos, const int32_t* m
           "stage material");
   }
   JF_CK(jf_load_launch(e, m, n), "load kernel");
+  if (e->d_order) {
+    // clusters take instances in descending live count, so that the longest
+    // run first when the clusters do not all fit at once
+    int32_t live = 0;
+    for (int k = 0; k < n; ++k) live += material[k] >= 0 ? 1 : 0;
+    e->n_live[m] = live;
+    for (int q = 0; q < e->M; ++q) e->h_order[q] = q;
+    std::stable_sort(e->h_order.begin(), e->h_order.end(),
+                     [&](int32_t a, int32_t b) { return e->n_live[a] > e->n_live[b]; });
+    JF_CK(cudaMemcpyAsync(e->d_order, e->h_order.data(), sizeof(int32_t) * e->M, cudaMemcpyHostToDevice,
+                          e->stream), "cluster order");
+  }
   JF_CK(cudaStreamSynchronize(e->stream), "load sync");
   e->sorted = false;
   return JF_OK;

@@ -61,6 +61,9 @@ struct jf_engine {
   int32_t* d_ovcur = nullptr;      // batched path: M x cluster overflow list cursors
   int32_t* d_band = nullptr;       // batched path: M x (cluster + 1) particle ranges
   int32_t* d_cap = nullptr;        // batched path: per-instance particles per cell lane
+  int32_t* d_order = nullptr;      // batched path: cluster -> instance, most live particles first
+  std::vector<int32_t> n_live;     // live particles per instance at its last load
+  std::vector<int32_t> h_order;    // host copy of d_order
   int32_t cell_cap = 0;            // batched path: fixed cell cap, 0 = cost model per re-sort
   float4* d_grid = nullptr;        // grid nodes (node = g_off + j * nx + i): (v0, v1, m, 0)
   double* d_stats = nullptr;       // M x 6 CoM sums (payload y, count, x; body y, count, x)

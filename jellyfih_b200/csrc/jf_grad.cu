@@ -39,7 +39,8 @@ struct GradArgs {
   const JfInst* inst;
   const JfParams* params;
   JfMaterials mats;
-  GradState s;                 // the state the kernel reads (pre-step) and, forward, writes
+  GradState s;                 // the state the kernel reads (pre-step)
+  GradState o;                 // where it writes the post-step state (s itself in the forward)
   const int32_t* mat;
   float* Jp;
   const float2* fiber;
@@ -75,17 +76,24 @@ __global__ void gf_p2g(GradArgs a) {
   if (k >= I.n_slots) return;
   const int64_t g = I.p_off + k;
   const int mt = a.mat[g];
-  if (mt < 0) return;
+  const bool copy = a.o.F != a.s.F;
+  if (mt < 0) {
+    if (copy) a.o.F[g] = a.s.F[g];
+    return;
+  }
   const float4 xv = a.s.xv[g];
   JfStencil st;
-  if (!jf_stencil(I, make_float2(xv.x, xv.y), st)) return;
+  if (!jf_stencil(I, make_float2(xv.x, xv.y), st)) {
+    if (copy) a.o.F[g] = a.s.F[g];
+    return;
+  }
   float4 F = a.s.F[g];
   float jp = (mt == 2) ? a.Jp[g] : 1.0f;
   const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
   JfScatter sc;
   jf_p2g_particle(I, a.mats, mt, make_float2(xv.z, xv.w), a.s.C[g], F, jp, fb, pressure,
                   a.params[m].payload_density, sc);
-  a.s.F[g] = F;
+  a.o.F[g] = F;
   if (mt == 2) a.Jp[g] = jp;
   unsigned long long* fix = a.fix + 3 * I.g_off;
 #pragma unroll
@@ -118,15 +126,21 @@ __global__ void gf_g2p(GradArgs a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= I.n_slots) return;
   const int64_t g = I.p_off + k;
-  if (a.mat[g] < 0) return;
+  if (a.mat[g] < 0) {
+    if (a.o.xv != a.s.xv) {
+      a.o.xv[g] = a.s.xv[g];
+      a.o.C[g] = a.s.C[g];
+    }
+    return;
+  }
   const float4 xv = a.s.xv[g];
   float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
   float4 C = a.s.C[g];
   const float2* u = a.u + I.g_off;
   const int nx = I.nx;
   jf_g2p_particle(I, x, v, C, [&](int ni, int nj) { return u[nj * nx + ni]; });
-  a.s.xv[g] = make_float4(x.x, x.y, v.x, v.y);
-  a.s.C[g] = C;
+  a.o.xv[g] = make_float4(x.x, x.y, v.x, v.y);
+  a.o.C[g] = C;
 }
 
 struct AdjArgs {
@@ -280,14 +294,8 @@ __global__ void ad_p2g(AdjArgs A) {
         const float dt = I.dt;
         const float M00 = radd(1.0f, rmul(dt, C.x)), M01 = rmul(dt, C.y);
         const float M10 = rmul(dt, C.z), M11 = radd(1.0f, rmul(dt, C.w));
-        D4 Fs[4];
         const float fsv[4] = {rdot2(M00, F.x, M01, F.z), rdot2(M00, F.y, M01, F.w),
                               rdot2(M10, F.x, M11, F.z), rdot2(M10, F.y, M11, F.w)};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          Fs[q] = d4c(fsv[q]);
-          Fs[q].d[q] = 1.0f;
-        }
         const int ms = jf_mat_slot(mt);
         const JfMaterials& mats = a.mats;
         const float mu = ms == 0 ? mats.mu[0] : ms == 1 ? mats.mu[1] : ms == 2 ? mats.mu[2]
@@ -295,8 +303,35 @@ __global__ void ad_p2g(AdjArgs A) {
         const float la = ms == 0 ? mats.la[0] : ms == 1 ? mats.la[1] : ms == 2 ? mats.la[2]
                        : ms == 3 ? mats.la[3] : mats.la[4];
         const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+        // the material map F* -> (F_out, tau): values and Jacobians d./dF*[e]
         D4 Fo[4], tau[4], J;
-        jf_phi<D4>(Fs, mt, mu, la, pressure, fb, Fo, tau, J);
+        const JfSvdRot rot = jf_svd2_values(make_float4(fsv[0], fsv[1], fsv[2], fsv[3]));
+        if (mt == 0 && rot.s1 > 1e-6f && rot.s2 > 1e-6f) {
+          // water, no singular value at the 1e-6 floor: J = s1 s2 = det F*, so
+          // dJ = cof F*; F_out = sqrt(J) I, tau = lambda J (J - 1) I
+          // (mpm_sim.py:219-227 with mu = 0); values as the forward rounds them
+          const float Jw = rmul(rot.s1, rot.s2);
+          const float dJ[4] = {fsv[3], -fsv[2], -fsv[1], fsv[0]};
+          const float kf = 0.5f / sqrtf(Jw), kt = la * (2.0f * Jw - 1.0f);
+          const float sj = sqrtf(Jw), diag = rmul(rmul(la, Jw), rsub(Jw, 1.0f));
+          Fo[0] = d4c(sj); Fo[1] = d4c(0.0f); Fo[2] = d4c(0.0f); Fo[3] = d4c(sj);
+          tau[0] = d4c(diag); tau[1] = d4c(0.0f); tau[2] = d4c(0.0f); tau[3] = d4c(diag);
+          J = d4c(Jw);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            Fo[0].d[e] = Fo[3].d[e] = kf * dJ[e];
+            tau[0].d[e] = tau[3].d[e] = kt * dJ[e];
+            J.d[e] = dJ[e];
+          }
+        } else {
+          D4 Fs[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            Fs[q] = d4c(fsv[q]);
+            Fs[q].d[q] = 1.0f;
+          }
+          jf_phi<D4>(Fs, mt, mu, la, pressure, fb, Fo, tau, J);
+        }
         float mass = I.p_mass;
         if (mt == 2) mass = mass * a.params[m].payload_density;
         const float ks = I.stress_scale;
@@ -443,6 +478,7 @@ static GradArgs grad_args(jf_engine* e, GradState s, float t) {
   a.params = e->d_params;
   a.mats = jf_materials();
   a.s = s;
+  a.o = s;
   a.mat = e->p.mat;
   a.Jp = e->p.Jp;
   a.fiber = e->p.fiber;
@@ -466,12 +502,14 @@ static cudaError_t copy_state(jf_engine* e, GradState dst, GradState src) {
   return cudaMemcpyAsync(dst.F, src.F, bytes, cudaMemcpyDeviceToDevice, e->stream);
 }
 
-// one deterministic substep of every instance on state s at time t; with
-// u_keep / pmv_keep set, its grid is written there for the adjoint
+// one deterministic substep of every instance from state s at time t into
+// state o (s itself when o is not given); with u_keep / pmv_keep set, its grid
+// is written there for the adjoint
 static cudaError_t det_substep(jf_engine* e, GradState s, float t, float2* u_keep = nullptr,
-                               float4* pmv_keep = nullptr) {
+                               float4* pmv_keep = nullptr, const GradState* o = nullptr) {
   JfGrad* G = e->grad;
   GradArgs a = grad_args(e, s, t);
+  if (o) a.o = *o;
   if (u_keep) {
     a.u = u_keep;
     a.pmv = pmv_keep;
@@ -575,12 +613,15 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   for (int64_t seg = n_seg - 1; seg >= 0; --seg) {
     const int64_t s0 = seg * K;
     const int n = (int)((steps - s0) < K ? (steps - s0) : K);
-    if ((err = copy_state(e, work, state_at(G->ck, slots, (size_t)seg))) != cudaSuccess) return err;
+    // the segment's pre-step states: substep j reads seg[j] and writes seg[j + 1]
+    if ((err = copy_state(e, state_at(G->seg, slots, 0), state_at(G->ck, slots, (size_t)seg))) != cudaSuccess)
+      return err;
     const size_t nodes = (size_t)e->total_nodes;
     for (int j = 0; j < n; ++j) {
-      if ((err = copy_state(e, state_at(G->seg, slots, (size_t)j), work)) != cudaSuccess) return err;
       JfTimed timed(e, true);
-      if ((err = det_substep(e, work, ts[s0 + j], G->useg + nodes * j, G->pmseg + nodes * j)) != cudaSuccess)
+      const GradState next = (j + 1 < n) ? state_at(G->seg, slots, (size_t)j + 1) : work;
+      if ((err = det_substep(e, state_at(G->seg, slots, (size_t)j), ts[s0 + j], G->useg + nodes * j,
+                             G->pmseg + nodes * j, &next)) != cudaSuccess)
         return err;
     }
     for (int j = n - 1; j >= 0; --j) {

@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--no-refine", action="store_true", help="skip the 256 x 64^2 gradient-refinement leg")
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiable leg (8 of the workload's instances) and print it")
     return ap.parse_args()
@@ -225,6 +226,56 @@ def uneven_leg(device, stream, substeps=256):
     out["autotuned"] = dict(best, value=timed(best["resort_interval"], best["cluster_size"]))
     out["unit"] = UNIT
     return out
+
+
+def refine_leg(device, stream, M=256, steps=400, iterations=3, checkpoint_every=50):
+    """The gradient-refined search step of the 256 x 64^2 configuration (dx = 1/64,
+    20,000 slots, ~14.9K live), on a bounded sample of its 4,000-substep horizon:
+    genomes from a seeded Gaussian (CMA-ES style) sample, `iterations` gradient
+    steps of 0.05 of the range on the two timing genes (each a checkpointed
+    forward + backward of all instances), then the initial and refined genomes
+    re-judged by the plain forward path and the GPU fitness kernel."""
+    import torch
+    from jellyfih_b200 import Engine, InstanceSpec, tank
+    from jellyfih_b200.autograd import refine_timing_genes
+    genomes = tank.gaussian_genomes(M, 5000)
+    data = [tank.fill_tank(g, 20000, grid_res=64) for g in genomes]
+    pos = [d[0] for d in data]
+    mats = [d[1] for d in data]
+    fibs = [d[2] for d in data]
+    muscle = np.array([d[3]["muscle_count"] for d in data], np.int32)
+    spec = InstanceSpec(20000, 64, 64, 1.0)
+    e = Engine([spec] * M, path="plain", device=device)
+    e.set_stream(stream)
+    refine_timing_genes(e, genomes, pos, mats, fibs, steps, 1, checkpoint_every=checkpoint_every)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    refined, hist = refine_timing_genes(e, genomes, pos, mats, fibs, steps, iterations,
+                                        checkpoint_every=checkpoint_every)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e.close()
+
+    judge = Engine([spec] * M, path="plain", device=device)
+    judge.set_stream(stream)
+    fits = {}
+    for name, g in (("initial", genomes), ("refined", refined)):
+        for m in range(M):
+            judge.load(m, pos[m], mats[m], fibs[m])
+        c = np.clip(g[:, 9], 0.05, 0.60)
+        judge.set_params(contraction=c, freq=np.clip(g[:, 10], 0.5, 2.0))
+        rows = judge.run_headless(steps)
+        fits[name] = {"mean_displacement": float(np.mean(rows[:, 2] - rows[:, 0])),
+                      "fitness": judge.fitness(rows, muscle, c, mode="displacement")}
+    judge.close()
+    better = float(np.mean(fits["refined"]["fitness"] < fits["initial"]["fitness"]))
+    return {"instances": M, "grid": "64x64", "slots": 20000, "live_per_instance": float(np.mean([(m >= 0).sum() for m in mats])),
+            "substeps": steps, "checkpoint_every": checkpoint_every, "gradient_steps": iterations,
+            "s_per_gradient_step": wall / iterations,
+            "mean_displacement_per_step": [float(np.mean(h)) for h in hist],
+            "plain_judge": {"initial_mean_displacement": fits["initial"]["mean_displacement"],
+                            "refined_mean_displacement": fits["refined"]["mean_displacement"],
+                            "fraction_with_better_fitness": better}}
 
 
 def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
@@ -452,6 +503,8 @@ def run_ours(args):
                            "batched_over_plain": value / plain_value}
 
         extras["differentiable"] = grad_leg(inputs[:8], local, stream)
+        if not args.no_refine:
+            extras["refine"] = refine_leg(local, stream)
 
         if not args.no_uneven:
             extras["uneven"] = uneven_leg(local, stream)
@@ -487,7 +540,10 @@ def run_grad_only(args):
     torch.cuda.set_device(0)
     inputs = make_inputs(args.instances, args.slots, 1000)
     stream = torch.cuda.Stream()
-    print(json.dumps({"differentiable": grad_leg(inputs[:8], 0, stream)}), flush=True)
+    out = {"differentiable": grad_leg(inputs[:8], 0, stream)}
+    if not args.no_refine:
+        out["refine"] = refine_leg(0, stream)
+    print(json.dumps(out), flush=True)
     return 0
 
 

@@ -454,30 +454,31 @@ def run_ours(args):
         extras["graphs"] = {"value": live_total * 2 * S / (gms / 1e3), "unit": UNIT,
                             "steps": 2, "note": "two more bench steps, graphs replayed, kernel timing off"}
 
-        # e2e through the public API: host (pinned) inputs in, (M, 5) results out, every step
-        pinned = []
-        for pos, mat, fib, c, f, st in inputs:
-            hp = torch.from_numpy(pos).pin_memory().numpy()
-            hm = torch.from_numpy(mat).pin_memory().numpy()
-            hf = torch.from_numpy(fib).pin_memory().numpy()
-            pinned.append((hp, hm, hf, c, f))
-        h2d = sum(a.nbytes + b.nbytes + c.nbytes for a, b, c, _, _ in pinned)
+        # e2e through the public API: one evaluation episode per step (jf_run_episode:
+        # every instance loaded from pinned host arrays, run_headless, GPU fitness,
+        # (M, 5) rows and (M,) fitness read back)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        pos_all = pin(np.concatenate([i[0] for i in inputs]))
+        mat_all = pin(np.concatenate([i[1] for i in inputs]))
+        fib_all = pin(np.concatenate([i[2] for i in inputs]))
+        con = np.array([i[3] for i in inputs], np.float32)
+        frq = np.array([i[4] for i in inputs], np.float32)
+        mus = np.array([i[5]["muscle_count"] for i in inputs], np.int32)
+        h2d = pos_all.nbytes + mat_all.nbytes + fib_all.nbytes + con.nbytes + frq.nbytes + mus.nbytes
         e2e_steps = max(2, K // 4)
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            for m, (hp, hm, hf, c, f) in enumerate(pinned):
-                engine.load(m, hp, hm, hf)
-            engine.set_params(contraction=[p[3] for p in pinned], freq=[p[4] for p in pinned])
-            res = engine.run_headless(S)
+            res, fit = engine.run_episode(pos_all, mat_all, con, S, fibers=fib_all, freq=frq, muscle_counts=mus)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
         barrier()
         el = allreduce(el, dist.ReduceOp.MAX if world > 1 else None)
         extras["e2e"] = {"value": live_total * S * e2e_steps / el, "unit": UNIT,
-                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": res.nbytes + 2 * 6 * 8 * M,
-                         "steps": e2e_steps, "api": "Engine.load + Engine.run_headless (C ABI)"}
+                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": res.nbytes + fit.nbytes,
+                         "steps": e2e_steps,
+                         "api": "Engine.run_episode (jf_run_episode: loads, headless run, GPU fitness)"}
         if world > 1:
             from jellyfih_b200.shard import gather_rows
             extras["e2e"]["gathered_results"] = int(gather_rows(res).shape[0])

@@ -132,6 +132,21 @@ int jf_run_headless(jf_engine* e, int64_t steps, double* out);
 int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts,
                const double* contraction, int32_t mode, double* out);
 
+/* One evaluation episode of every instance with a single host round trip,
+ * the loop body of evolve.py:127-155 and 90-124: load_particles for every
+ * instance (mpm_sim.py:715-736), instance_act_contraction / instance_freq
+ * set, run_batch_headless(steps) (:802-834), then compute_fitness on the GPU.
+ * pos [total slots][2], material [total slots], fiber [total slots][2] (NULL:
+ * (0, 1)) hold the instances' slot arrays back to back (instance m's
+ * n_slots entries after those of instances 0 .. m-1; material -1 = empty
+ * slot).  contraction, freq: [n_instances] (freq NULL keeps the current
+ * values).  rows: [n_instances][5] as jf_run_headless.  muscle_counts NULL
+ * skips the fitness; else fitness [n_instances] as jf_fitness in `mode`
+ * with contraction as the gene.  One synchronisation at the end. */
+int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, const float* fiber,
+                   const float* contraction, const float* freq, int64_t steps,
+                   const int32_t* muscle_counts, int32_t mode, double* rows, double* fitness);
+
 /* Differentiable rollout.  jf_grad_forward runs `steps` substeps from the
  * current state with a deterministic P2G, checkpointing (x, v, C, F) every
  * `checkpoint_every` substeps, and returns loss[m] = the displacement of the

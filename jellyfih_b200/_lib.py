@@ -57,6 +57,7 @@ EXPORTS = {
     "jf_stats_raw": (ctypes.c_int, [_E, _P]),
     "jf_run_headless": (ctypes.c_int, [_E, ctypes.c_int64, _P]),
     "jf_fitness": (ctypes.c_int, [_E, _P, _P, _P, ctypes.c_int32, _P]),
+    "jf_run_episode": (ctypes.c_int, [_E, _P, _P, _P, _P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P]),
     "jf_grad_forward": (ctypes.c_int, [_E, ctypes.c_int64, ctypes.c_int32, _P]),
     "jf_grad_backward": (ctypes.c_int, [_E, _P, _P, _P]),
     "jf_grad_positions": (ctypes.c_int, [_E, ctypes.c_int32, _P]),

@@ -389,7 +389,8 @@ int jf_destroy(jf_engine* e) {
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_rank); cudaFree(e->d_ovlist); cudaFree(e->d_ovband); cudaFree(e->d_ovcur);
-  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
+  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_ep); cudaFree(e->d_ep_mat);
+  cudaFree(e->d_ep_stats); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
@@ -575,6 +576,83 @@ int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts
   JF_CK(jf_fitness_launch(e, d_rows, d_mus, contraction ? d_con : nullptr, mode, d_out), "fitness kernel");
   JF_CK(cudaMemcpyAsync(out, d_out, sizeof(double) * M, cudaMemcpyDeviceToHost, e->stream), "fitness read");
   JF_CK(cudaStreamSynchronize(e->stream), "fitness sync");
+  return JF_OK;
+}
+
+int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, const float* fiber,
+                   const float* contraction, const float* freq, int64_t steps,
+                   const int32_t* muscle_counts, int32_t mode, double* rows, double* fitness) {
+  if (check_engine(e) || !pos || !material || !contraction || !rows) return JF_ERR_INVALID;
+  if (steps < 0) return fail(e, JF_ERR_INVALID, "steps must be >= 0");
+  if (muscle_counts && !fitness) return fail(e, JF_ERR_INVALID, "fitness output required with muscle_counts");
+  if (mode != 0 && mode != 1) return fail(e, JF_ERR_INVALID, "fitness mode must be 0 or 1");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const size_t S = (size_t)e->total_slots, M = (size_t)e->M;
+  if (!e->d_ep) {
+    cudaError_t err;
+    if ((err = cudaMalloc((void**)&e->d_ep, sizeof(float) * 5 * (S > 0 ? S : 1))) != cudaSuccess ||
+        (err = cudaMalloc((void**)&e->d_ep_mat, sizeof(int32_t) * (S > 0 ? S : 1))) != cudaSuccess ||
+        (err = cudaMalloc((void**)&e->d_ep_stats, sizeof(double) * 6 * M)) != cudaSuccess)
+      return cuda_fail(e, err, "episode staging");
+  }
+  float* d_pos = e->d_ep;
+  float* d_fib = e->d_ep + 2 * S;
+  float* d_glow = e->d_ep + 4 * S;
+  // loads of every instance (mpm_sim.py:715-727), one copy per array
+  if (S > 0) {
+    JF_CK(cudaMemcpyAsync(d_pos, pos, sizeof(float) * 2 * S, cudaMemcpyHostToDevice, e->stream), "episode pos");
+    JF_CK(cudaMemcpyAsync(e->d_ep_mat, material, sizeof(int32_t) * S, cudaMemcpyHostToDevice, e->stream),
+          "episode material");
+    if (fiber)
+      JF_CK(cudaMemcpyAsync(d_fib, fiber, sizeof(float) * 2 * S, cudaMemcpyHostToDevice, e->stream), "episode fiber");
+  }
+  JF_CK(jf_load_all_launch(e, d_pos, e->d_ep_mat, fiber ? d_fib : nullptr, d_glow), "episode load");
+  e->sorted = false;
+  if (e->d_order) {
+    for (size_t m = 0; m < M; ++m) {
+      const JfInst& I = e->inst[m];
+      int32_t live = 0;
+      for (int32_t k = 0; k < I.n_slots; ++k) live += material[I.p_off + k] >= 0 ? 1 : 0;
+      e->n_live[m] = live;
+    }
+    for (size_t q = 0; q < M; ++q) e->h_order[q] = (int32_t)q;
+    std::stable_sort(e->h_order.begin(), e->h_order.end(),
+                     [&](int32_t a, int32_t b) { return e->n_live[a] > e->n_live[b]; });
+    JF_CK(cudaMemcpyAsync(e->d_order, e->h_order.data(), sizeof(int32_t) * M, cudaMemcpyHostToDevice, e->stream),
+          "cluster order");
+  }
+  // timing genes (evolve.py:150-152)
+  for (size_t m = 0; m < M; ++m) {
+    e->params[m].contraction = contraction[m];
+    if (freq) e->params[m].freq = freq[m];
+  }
+  e->params_dirty = true;
+  // run_batch_headless (mpm_sim.py:802-834) with the rows formed on the device
+  e->t = 0.0f;
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  JF_CK(cudaMemcpyAsync(e->d_ep_stats, e->d_stats, sizeof(double) * 6 * M, cudaMemcpyDeviceToDevice, e->stream),
+        "stats before");
+  if ((rc = step_impl(e, steps))) return rc;
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  double* d_rows = e->d_fit;          // 5M doubles
+  double* d_out = e->d_fit + 5 * M;   // M doubles
+  JF_CK(jf_rows_launch(e, e->d_ep_stats, e->d_stats, d_rows), "rows kernel");
+  if (muscle_counts) {
+    std::vector<double> con(M);
+    for (size_t m = 0; m < M; ++m) con[m] = (double)contraction[m];
+    JF_CK(cudaMemcpyAsync(e->d_fit_i, muscle_counts, sizeof(int32_t) * M, cudaMemcpyHostToDevice, e->stream),
+          "fitness counts");
+    JF_CK(cudaMemcpyAsync(e->d_fit_f, con.data(), sizeof(double) * M, cudaMemcpyHostToDevice, e->stream),
+          "fitness genes");
+    JF_CK(jf_fitness_launch(e, d_rows, e->d_fit_i, e->d_fit_f, mode, d_out), "fitness kernel");
+    JF_CK(cudaMemcpyAsync(fitness, d_out, sizeof(double) * M, cudaMemcpyDeviceToHost, e->stream), "fitness read");
+    JF_CK(cudaMemcpyAsync(rows, d_rows, sizeof(double) * 5 * M, cudaMemcpyDeviceToHost, e->stream), "rows read");
+    JF_CK(cudaStreamSynchronize(e->stream), "episode sync");
+  } else {
+    JF_CK(cudaMemcpyAsync(rows, d_rows, sizeof(double) * 5 * M, cudaMemcpyDeviceToHost, e->stream), "rows read");
+    JF_CK(cudaStreamSynchronize(e->stream), "episode sync");
+  }
   return JF_OK;
 }
 

@@ -62,6 +62,9 @@ struct jf_engine {
   int32_t* d_band = nullptr;       // batched path: M x (cluster + 1) particle ranges
   int32_t* d_cap = nullptr;        // batched path: per-instance particles per cell lane
   int32_t* d_order = nullptr;      // batched path: cluster -> instance, most live particles first
+  float* d_ep = nullptr;           // episode staging: pos (2), fiber (2), glow (1) floats per slot
+  int32_t* d_ep_mat = nullptr;     // episode staging: material per slot
+  double* d_ep_stats = nullptr;    // episode: CoM sums before the run (6 per instance)
   std::vector<int32_t> n_live;     // live particles per instance at its last load
   std::vector<int32_t> h_order;    // host copy of d_order
   int32_t cell_cap = 0;            // batched path: fixed cell cap, 0 = cost model per re-sort
@@ -122,6 +125,12 @@ cudaError_t jf_plain_step(jf_engine* e, int64_t n_steps);
 cudaError_t jf_batched_step(jf_engine* e, int64_t n_steps);
 cudaError_t jf_batched_sort(jf_engine* e);
 size_t jf_batched_smem_bytes(const jf_engine* e);
+
+// Episode helpers (jf_run_episode): load every instance from slot-ordered
+// staging, and the (M, 5) rows from before / after CoM sums, on the device.
+cudaError_t jf_load_all_launch(jf_engine* e, const float* d_pos, const int32_t* d_mat, const float* d_fib,
+                               float* d_glow_slot);
+cudaError_t jf_rows_launch(jf_engine* e, const double* d_before, const double* d_after, double* d_rows);
 
 // Fitness of every instance from (M, 5) rows on the device (FP64).
 cudaError_t jf_fitness_launch(jf_engine* e, const double* d_rows, const int32_t* d_muscle,

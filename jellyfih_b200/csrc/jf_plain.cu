@@ -152,6 +152,60 @@ __global__ void load_kernel(JfInst I, int32_t n, const float* __restrict__ pos,
   p.rref[g] = x.x;  // mpm_sim.py:727
 }
 
+// Every instance at once (blockIdx.y = instance) from slot-ordered staging
+// laid out as the engine's slots: the same reset as load_kernel.
+__global__ void load_all_kernel(const JfInst* __restrict__ inst, const float* __restrict__ pos,
+                                const int32_t* __restrict__ mt_in, const float* __restrict__ fib,
+                                int has_fiber, JfParticles p, const float* __restrict__ glow_slot) {
+  const JfInst I = inst[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  const int mt = mt_in[g];
+  const float2 x = make_float2(pos[2 * g], pos[2 * g + 1]);
+  p.xv[g] = make_float4(x.x, x.y, 0.0f, 0.0f);
+  p.C[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  p.F[g] = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
+  p.mat[g] = mt;
+  p.fiber[g] = has_fiber ? make_float2(fib[2 * g], fib[2 * g + 1]) : make_float2(0.0f, 1.0f);
+  p.Jp[g] = 1.0f;
+  p.glow[g] = glow_slot[g];
+  p.slot[g] = k;
+  p.rref[g] = x.x;  // mpm_sim.py:727
+}
+
+// glow of every instance into slot order (blockIdx.y = instance)
+__global__ void glow_all_to_slot_kernel(const JfInst* __restrict__ inst, const float* __restrict__ glow,
+                                        const int32_t* __restrict__ slot, float* __restrict__ out) {
+  const JfInst I = inst[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  out[I.p_off + slot[g]] = glow[g];
+}
+
+// run_batch_headless rows (mpm_sim.py:776-834) from the CoM sums before and
+// after: the payload CoM, or the jelly + muscle CoM without payload;
+// [init_y, init_x, final_y, final_x, final_y >= 0.01], zeros without either.
+__global__ void rows_kernel(int M, const double* __restrict__ before, const double* __restrict__ after,
+                            double* __restrict__ rows) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  const double* a = before + 6 * (size_t)m;
+  const double* b = after + 6 * (size_t)m;
+  if (a[1] == 0) a += 3;
+  if (b[1] == 0) b += 3;
+  double* o = rows + 5 * (size_t)m;
+  o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
+  if (a[1] > 0 && b[1] > 0) {
+    o[0] = a[0] / a[1];
+    o[1] = a[2] / a[1];
+    o[2] = b[0] / b[1];
+    o[3] = b[2] / b[1];
+    o[4] = (o[2] < 0.01) ? 0.0 : 1.0;
+  }
+}
+
 __global__ void glow_to_slot_kernel(JfInst I, const float* __restrict__ glow,
                                     const int32_t* __restrict__ slot, float* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,6 +324,23 @@ cudaError_t jf_fitness_launch(jf_engine* e, const double* d_rows, const int32_t*
                               const double* d_contraction, int mode, double* d_out) {
   fitness_kernel<<<1, 1024, 0, e->stream>>>(e->d_inst, e->M, d_rows, d_muscle, d_contraction,
                                             d_contraction != nullptr, mode, d_out);
+  e->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_load_all_launch(jf_engine* e, const float* d_pos, const int32_t* d_mat, const float* d_fib,
+                               float* d_glow_slot) {
+  if (e->max_slots == 0) return cudaSuccess;
+  const dim3 grid(blocks_for(e->max_slots), e->M);
+  glow_all_to_slot_kernel<<<grid, kThreads, 0, e->stream>>>(e->d_inst, e->p.glow, e->p.slot, d_glow_slot);
+  load_all_kernel<<<grid, kThreads, 0, e->stream>>>(e->d_inst, d_pos, d_mat, d_fib, d_fib != nullptr, e->p,
+                                                    d_glow_slot);
+  e->launches += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t jf_rows_launch(jf_engine* e, const double* d_before, const double* d_after, double* d_rows) {
+  rows_kernel<<<(e->M + 127) / 128, 128, 0, e->stream>>>(e->M, d_before, d_after, d_rows);
   e->launches += 1;
   return cudaGetLastError();
 }

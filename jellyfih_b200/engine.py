@@ -192,6 +192,32 @@ class Engine:
                                          {"efficiency": 0, "displacement": 1}[mode], _ptr(out)))
         return out
 
+    def run_episode(self, positions, materials, contraction, steps: int, fibers=None, freq=None,
+                    muscle_counts=None, mode: str = "efficiency"):
+        """One evaluation episode of every instance with one host round trip:
+        load every instance, set the timing genes, run_headless(steps), and
+        (with muscle_counts) the GPU fitness.  positions / materials / fibers:
+        per-instance slot arrays (lists) or the instances' arrays back to back.
+        Returns (rows (M, 5), fitness (M,) or None)."""
+        S = sum(s.n_slots for s in self.instances)
+        cat = lambda a, dt, w: np.ascontiguousarray(  # noqa: E731
+            np.concatenate([np.asarray(x, dt).reshape(-1, w) for x in a]) if isinstance(a, (list, tuple))
+            else np.asarray(a, dt).reshape(-1, w), dtype=dt)
+        pos = cat(positions, np.float32, 2)
+        mat = cat(materials, np.int32, 1).reshape(-1)
+        if pos.shape[0] != S or mat.shape[0] != S:
+            raise ValueError(f"positions and materials must cover all {S} slots")
+        fib = None if fibers is None else cat(fibers, np.float32, 2)
+        con = np.ascontiguousarray(contraction, dtype=np.float32).reshape(self.M)
+        frq = None if freq is None else np.ascontiguousarray(freq, dtype=np.float32).reshape(self.M)
+        mus = None if muscle_counts is None else np.ascontiguousarray(muscle_counts, dtype=np.int32).reshape(self.M)
+        rows = np.zeros((self.M, 5), np.float64)
+        fit = None if mus is None else np.zeros(self.M, np.float64)
+        self._check(self._lib.jf_run_episode(self._h, _ptr(pos), _ptr(mat), _ptr(fib), _ptr(con), _ptr(frq),
+                                             int(steps), _ptr(mus), {"efficiency": 0, "displacement": 1}[mode],
+                                             _ptr(rows), _ptr(fit)))
+        return rows, fit
+
     # -- differentiable rollout -----------------------------------------------
     def grad_forward(self, steps: int, checkpoint_every: int = 100) -> np.ndarray:
         """Rollout with checkpoints; returns the (M,) CoM displacement (the loss)."""

@@ -367,6 +367,44 @@ def test_axisym_rejected_by_the_differentiable_rollout():
         e.grad_forward(4, 2)
     e.close()
 
+
+@pytest.mark.parametrize("path", PATHS)
+def test_run_episode_matches_separate_calls(path):
+    """jf_run_episode (one round trip) against load / set_params /
+    run_headless / fitness called one by one: equal at 0 substeps, equal up
+    to float-atomic summation order after 100."""
+    from jellyfih_b200 import InstanceSpec, tank
+    gs = tank.uniform_genomes(3, 21)
+    data = [tank.fill_tank(g, 12000, grid_res=64) for g in gs]
+    specs = [InstanceSpec(12000, 64, 64, 1.0)] * 3
+    pos = [d[0] for d in data]
+    mat = [d[1] for d in data]
+    fib = [d[2] for d in data]
+    mus = np.array([max(d[3]["muscle_count"], 250) for d in data], np.int32)
+    con = np.array([0.3, 0.45, 0.2], np.float32)
+    frq = np.array([1.0, 1.4, 0.8], np.float32)
+    for steps in (0, 100):
+        a = _engine(specs, path)
+        rows_a, fit_a = a.run_episode(pos, mat, con, steps, fibers=fib, freq=frq, muscle_counts=mus)
+        b = _engine(specs, path)
+        for m in range(3):
+            b.load(m, pos[m], mat[m], fib[m])
+        b.set_params(contraction=con, freq=frq)
+        rows_b = b.run_headless(steps)
+        fit_b = b.fitness(rows_b, mus, con.astype(np.float64))
+        if steps == 0:
+            assert np.array_equal(rows_a, rows_b)
+            assert np.array_equal(fit_a, fit_b)
+        else:
+            np.testing.assert_allclose(rows_a, rows_b, rtol=1e-6, atol=1e-7)
+            np.testing.assert_allclose(fit_a, fit_b, rtol=1e-2, atol=1e-4)
+        assert a.time == b.time
+        ra, rb = a.read(1), b.read(1)
+        np.testing.assert_allclose(ra["x"], rb["x"], atol=1e-5)
+        assert np.array_equal(ra["material"], rb["material"])
+        a.close()
+        b.close()
+
 def test_graph_replay_matches_direct_launches():
     """Chunks replayed from a CUDA graph give the direct launches' results."""
     from jellyfih_b200 import InstanceSpec

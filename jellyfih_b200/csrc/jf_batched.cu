@@ -209,8 +209,10 @@ __device__ __forceinline__ void flush_block(const float* acc, const Window& w, i
 __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
-  __shared__ float s_pressure;
-  __shared__ int s_next_task;
+  // per-substep values, double-buffered so that substep s + 1's are set
+  // before the barrier that ends substep s
+  __shared__ float s_pressure[2];
+  __shared__ int s_next_task[2];
 
   cg::cluster_group cluster = cg::this_cluster();
   const int CS = a.CS;
@@ -304,18 +306,26 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const int n_gen_tasks = (n_generic_all + 31) >> 5;
   const int n_tasks = n_cell_tasks + n_gen_tasks;
 
+  // window rows outside the band (pushed to / pulled from their owners):
+  // row 0 and rows n_own + 1 .. WR - 1
+  const int n_own = max(own_hi - row0, 0);
+  const int n_halo_rows = w.WR - n_own;
+  const bool rows_by_thread = (nth % nx) == 0;  // the grid update can step whole rows
+
   float t = *a.t_dev;
+  if (tid == 0) {
+    s_pressure[0] = P.actuation * jf_activation(P.freq, P.contraction, t);
+    s_next_task[0] = n_warps;
+  }
+  __syncthreads();
   for (int s = 0; s <= a.K; ++s) {
     const bool do_g2p = s > 0;
     const bool do_p2g = s < a.K;
-    if (tid == 0) s_pressure = P.actuation * jf_activation(P.freq, P.contraction, t);
-    __syncthreads();
-    const float pressure = s_pressure;
+    const float pressure = s_pressure[s & 1];
+    int* next_task = &s_next_task[s & 1];
 
     // cells of the band: a warp takes 32 consecutive cells of one row; warps
     // claim row segments from a shared counter so that they finish together
-    if (tid == 0) s_next_task = n_warps;
-    __syncthreads();
     for (int task_id = warp; task_id < n_tasks;) {
       if (task_id < n_gen_tasks) {
         const int e = task_id + lane * n_gen_tasks;
@@ -326,7 +336,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           n_generic += over ? 0u : 1u;
         }
         int nt = 0;
-        if (lane == 0) nt = atomicAdd(&s_next_task, 1);
+        if (lane == 0) nt = atomicAdd(next_task, 1);
         task_id = __shfl_sync(0xffffffffu, nt, 0);
         continue;
       }
@@ -422,17 +432,19 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       __syncwarp();
       if (do_p2g) flush_block(acc, w, lane, cx, cy, seg0, nx);
       int nt = 0;
-      if (lane == 0) nt = atomicAdd(&s_next_task, 1);
+      if (lane == 0) nt = atomicAdd(next_task, 1);
       task_id = __shfl_sync(0xffffffffu, nt, 0);
     }
     __syncthreads();
 
     if (do_p2g) {
       // halo rows of the accumulator go to the rows' owners
-      for (int n = tid; n < WN; n += nth) {
-        const int wr = n / nx;
+      for (int q = tid; q < n_halo_rows * nx; q += nth) {
+        const int h = q / nx;
+        const int wr = h == 0 ? 0 : n_own + h;
         const int j = w.win0 + wr;
-        if ((j >= row0 && j < own_hi) || j < 0 || j >= ny) continue;
+        if (j < 0 || j >= ny) continue;
+        const int n = wr * nx + (q - h * nx);
         const float vx = w.Ax[n], vy = w.Ay[n], vm = w.Am[n];
         const float vh = I.axisym ? w.Ah[n] : 0.0f;
         if (vx != 0.0f || vy != 0.0f || vm != 0.0f || vh != 0.0f) {
@@ -452,12 +464,10 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       }
       cluster.sync();
 
-      // grid update of the owned rows; the accumulator is cleared for the next pass
+      // grid update of the owned rows (window rows 1 .. n_own); the
+      // accumulator is cleared for the next pass
       const bool last = (s == a.K - 1);
-      const int n_end = (kHaloLo + own_hi - row0) * nx;
-      for (int n = kHaloLo * nx + tid; n < n_end; n += nth) {
-        const int wr = n / nx;
-        const int i = n - wr * nx;
+      auto update_node = [&](int n, int wr, int i) {
         const int j = w.win0 + wr;
         const float mm = w.Am[n];
         const float2 u = jf_grid_node(I, i, j, w.Ax[n], w.Ay[n], mm, I.axisym ? w.Ah[n] : 0.0f);
@@ -468,21 +478,37 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         w.Ay[n] = 0.0f;
         w.Am[n] = 0.0f;
         if (I.axisym) w.Ah[n] = 0.0f;
+      };
+      if (rows_by_thread) {
+        // a thread keeps one column and steps nth / nx rows at a time
+        const int i = tid % nx, row_step = nth / nx;
+        for (int wr = kHaloLo + tid / nx; wr < kHaloLo + n_own; wr += row_step) update_node(wr * nx + i, wr, i);
+      } else {
+        for (int n = kHaloLo * nx + tid; n < (kHaloLo + n_own) * nx; n += nth) {
+          const int wr = n / nx;
+          update_node(n, wr, n - wr * nx);
+        }
       }
       cluster.sync();
 
       // halo rows of the updated grid come from their owners
-      for (int n = tid; n < WN; n += nth) {
-        const int wr = n / nx;
+      for (int q = tid; q < n_halo_rows * nx; q += nth) {
+        const int h = q / nx;
+        const int wr = h == 0 ? 0 : n_own + h;
         const int j = w.win0 + wr;
-        if ((j >= row0 && j < own_hi) || j < 0 || j >= ny) continue;
+        if (j < 0 || j >= ny) continue;
+        const int n = wr * nx + (q - h * nx);
         const int o = owner_of(w, j);
         const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
         w.Gx[n] = cluster.map_shared_rank(w.Gx, o)[rn];
         w.Gy[n] = cluster.map_shared_rank(w.Gy, o)[rn];
       }
-      __syncthreads();
       t = t + a.dt;
+      if (tid == 0) {
+        s_pressure[(s + 1) & 1] = P.actuation * jf_activation(P.freq, P.contraction, t);
+        s_next_task[(s + 1) & 1] = n_warps;
+      }
+      __syncthreads();
     }
   }
   // path counters: one atomic per warp

@@ -36,6 +36,12 @@ constexpr int kScanThreads = 1024;
 // caps 1 .. kCapCandidates - 1 and "no cap".
 constexpr int kCapCandidates = 16;
 constexpr int kMaxCluster = 16;
+// Band boundaries follow the particles: at each re-sort the rows are split
+// into CS bands of about equal cost (cell-loop iterations at the chosen cap,
+// overflow, grid update), each at most band_cap rows (the shared-memory
+// window's capacity).  Grids taller than kMaxBandRows keep equal-height bands.
+constexpr int kMaxBandRows = 1024;
+constexpr int kRowCost = 40;  // grid update of one row, in the cost model's units
 constexpr int kNoCap = 1 << 30;
 
 // Sort cell of a particle: (floor(X - 1/4), floor(Y - 1/4)) in grid units,
@@ -67,6 +73,7 @@ struct ChunkArgs {
   const int32_t* ovlist;      // overflow positions (relative to p_off), grouped by band
   const int32_t* ovband;      // M x (CS + 1): band starts in ovlist
   const int32_t* order;       // cluster -> instance
+  const int32_t* brow;        // M x (CS + 1): band row starts
   int32_t stride;
   float4* grid;             // grid of the chunk's last substep, node = g_off + j * nx + i
   int32_t* err;
@@ -85,11 +92,17 @@ struct ChunkArgs {
 // are reached in the owner CTA's window.
 struct Window {
   float *Gx, *Gy, *Ax, *Ay, *Am, *Ah;
-  int nx, H, win0, WR;
+  int nx, win0, WR, CS;
+  const int* brow;  // shared copy of the instance's band row starts (CS + 1)
 };
 
-__device__ __forceinline__ int owner_of(const Window& w, int j) { return j / w.H; }
-__device__ __forceinline__ int owner_row(const Window& w, int j, int o) { return j - (o * w.H - kHaloLo); }
+// the band (CTA of the cluster) that owns grid row j, and j's row in its window
+__device__ __forceinline__ int owner_of(const Window& w, int j) {
+  int o = 0;
+  while (o + 1 < w.CS && w.brow[o + 1] <= j) ++o;
+  return o;
+}
+__device__ __forceinline__ int owner_row(const Window& w, int j, int o) { return j - (w.brow[o] - kHaloLo); }
 
 __device__ __forceinline__ float2 gather_node(const Window& w, cg::cluster_group& cl, int i, int j) {
   const int wr = j - w.win0;
@@ -224,14 +237,18 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const JfInst I = a.inst[m];
   const JfParams P = a.params[m];
   const JfMaterials mats = a.mats;
-  const int nx = I.nx, ny = I.ny, H = I.band_h;
-  const int row0 = r * H;
-  const int own_hi = min(row0 + H, ny);
+  const int nx = I.nx, ny = I.ny;
+  __shared__ int s_brow[kMaxCluster + 1];
+  if (threadIdx.x <= CS) s_brow[threadIdx.x] = a.brow[m * (CS + 1) + threadIdx.x];
+  __syncthreads();
+  const int row0 = s_brow[r];
+  const int own_hi = s_brow[r + 1];
   Window w;
   w.nx = nx;
-  w.H = H;
+  w.CS = CS;
+  w.brow = s_brow;
   w.win0 = row0 - kHaloLo;
-  w.WR = H + kHalo;
+  w.WR = I.band_cap + kHalo;  // the window holds the largest band the sort may cut
   const int WN = w.WR * nx;
   w.Gx = sm;
   w.Gy = w.Gx + WN;
@@ -563,44 +580,47 @@ __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* 
 __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* __restrict__ inst,
                                                                 int32_t* __restrict__ counts,
                                                                 int stride, int32_t* __restrict__ band,
+                                                                int32_t* __restrict__ brow,
                                                                 int32_t* __restrict__ cap_out,
                                                                 int32_t* __restrict__ ovband,
                                                                 int32_t* __restrict__ ovcur, int CS,
                                                                 int fixed_cap) {
   __shared__ int warp_sums[kScanThreads / 32];
   __shared__ int s_cost[kCapCandidates];
-  __shared__ int s_band_over[kMaxCluster][kCapCandidates];
+  __shared__ int s_row_cost[kMaxBandRows];
+  __shared__ int s_row_over[kMaxBandRows];
+  __shared__ int s_brow[kMaxCluster + 1];
+  __shared__ int s_cap;
   const int m = blockIdx.x;
   const JfInst I = inst[m];
   const int cells = I.nx * I.ny;
   const int nbins = cells + 2;
   int32_t* c = counts + (int64_t)m * stride;
+  const int segs = (I.nx + 31) >> 5;
+  const bool dynamic = I.ny <= kMaxBandRows;
 
   // per-lane cap from the cell counts (candidate 0 = no cap); costs in
   // quarter lane-iterations: 128 per warp iteration, 6 per overflow particle
   if (threadIdx.x < kCapCandidates) s_cost[threadIdx.x] = 0;
-  for (int i = threadIdx.x; i < kMaxCluster * kCapCandidates; i += kScanThreads)
-    (&s_band_over[0][0])[i] = 0;
+  for (int y = threadIdx.x; y < min(I.ny, kMaxBandRows); y += kScanThreads) {
+    s_row_cost[y] = kRowCost;
+    s_row_over[y] = 0;
+  }
   __syncthreads();
-  {
-    const int segs = (I.nx + 31) >> 5;
-    for (int sg = threadIdx.x; sg < I.ny * segs; sg += kScanThreads) {
-      const int row = sg / segs;
-      const int x0 = (sg - row * segs) << 5;
-      const int xn = min(32, I.nx - x0);
-      const int32_t* cr = c + row * I.nx + x0;
-      int mx = 0;
-      for (int i = 0; i < xn; ++i) mx = max(mx, cr[i]);
-      if (mx == 0) continue;
-      const int br = min(row / I.band_h, CS - 1);
-      atomicAdd(&s_cost[0], 128 * mx);
-      for (int k = 1; k < kCapCandidates; ++k) {
-        int ov = 0;
-        if (k < mx)
-          for (int i = 0; i < xn; ++i) ov += max(0, cr[i] - k);
-        atomicAdd(&s_cost[k], 128 * min(mx, k) + 6 * ov);
-        if (ov) atomicAdd(&s_band_over[br][k], ov);
-      }
+  for (int sg = threadIdx.x; sg < I.ny * segs; sg += kScanThreads) {
+    const int row = sg / segs;
+    const int x0 = (sg - row * segs) << 5;
+    const int xn = min(32, I.nx - x0);
+    const int32_t* cr = c + row * I.nx + x0;
+    int mx = 0;
+    for (int i = 0; i < xn; ++i) mx = max(mx, cr[i]);
+    if (mx == 0) continue;
+    atomicAdd(&s_cost[0], 128 * mx);
+    for (int k = 1; k < kCapCandidates; ++k) {
+      int ov = 0;
+      if (k < mx)
+        for (int i = 0; i < xn; ++i) ov += max(0, cr[i] - k);
+      atomicAdd(&s_cost[k], 128 * min(mx, k) + 6 * ov);
     }
   }
   __syncthreads();
@@ -610,13 +630,70 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
       if (s_cost[k] < s_cost[best]) best = k;
     if (fixed_cap > 0) best = fixed_cap < kCapCandidates ? fixed_cap : 0;
     cap_out[m] = best == 0 ? kNoCap : best;
+    s_cap = best == 0 ? kNoCap : best;
+  }
+  __syncthreads();
+  // cost and overflow of every row at the chosen cap
+  const int cap = s_cap;
+  for (int sg = threadIdx.x; sg < I.ny * segs; sg += kScanThreads) {
+    const int row = sg / segs;
+    const int x0 = (sg - row * segs) << 5;
+    const int xn = min(32, I.nx - x0);
+    const int32_t* cr = c + row * I.nx + x0;
+    int mx = 0, ov = 0;
+    for (int i = 0; i < xn; ++i) {
+      mx = max(mx, cr[i]);
+      ov += max(0, cr[i] - cap);
+    }
+    if (dynamic) {
+      atomicAdd(&s_row_cost[row], 128 * min(mx, cap) + 6 * ov);
+      if (ov) atomicAdd(&s_row_over[row], ov);
+    } else if (ov) {
+      atomicAdd(&s_row_over[min(row / I.band_h, CS - 1)], ov);  // per band
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (dynamic) {
+      // band r starts where the prefix cost reaches r / CS of the total,
+      // clamped so that no band exceeds band_cap rows and the bands after it
+      // can still cover the rows that are left
+      long long total = 0;
+      for (int y = 0; y < I.ny; ++y) total += s_row_cost[y];
+      s_brow[0] = 0;
+      long long pre = 0;
+      int y = 0;
+      for (int r = 1; r < CS; ++r) {
+        const long long target = total * r / CS;
+        while (y < I.ny && pre + s_row_cost[y] / 2 < target) pre += s_row_cost[y++];
+        int b = y;
+        b = min(b, s_brow[r - 1] + I.band_cap);
+        b = max(b, I.ny - (CS - r) * I.band_cap);
+        b = max(b, s_brow[r - 1]);
+        b = min(b, I.ny);
+        while (y > b) pre -= s_row_cost[--y];
+        while (y < b) pre += s_row_cost[y++];
+        s_brow[r] = b;
+      }
+      s_brow[CS] = I.ny;
+    } else {
+      for (int r = 0; r < CS; ++r) s_brow[r] = min(r * I.band_h, I.ny);
+      s_brow[CS] = I.ny;
+    }
+    // overflow bins of the bands (in the position list order)
     int run = 0;
     for (int r = 0; r < CS; ++r) {
       ovband[m * (CS + 1) + r] = run;
       ovcur[m * CS + r] = run;
-      run += best == 0 ? 0 : s_band_over[r][best];
+      if (cap != kNoCap) {
+        if (dynamic)
+          for (int yy = s_brow[r]; yy < s_brow[r + 1]; ++yy) run += s_row_over[yy];
+        else
+          run += s_row_over[r];
+      }
     }
     ovband[m * (CS + 1) + CS] = run;
+    for (int r = 0; r <= CS; ++r) brow[m * (CS + 1) + r] = s_brow[r];
   }
   const int per = (nbins + kScanThreads - 1) / kScanThreads;
   const int b0 = threadIdx.x * per;
@@ -651,11 +728,7 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const int H = I.band_h;
-    for (int r = 0; r < CS; ++r) {
-      const int row = min(r * H, I.ny);
-      band[m * (CS + 1) + r] = (int32_t)I.p_off + c[row * I.nx];
-    }
+    for (int r = 0; r < CS; ++r) band[m * (CS + 1) + r] = (int32_t)I.p_off + c[s_brow[r] * I.nx];
     band[m * (CS + 1) + CS] = (int32_t)I.p_off + c[cells + 1];
   }
 }
@@ -665,8 +738,8 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
 __global__ void sort_scatter_kernel(const JfInst* __restrict__ inst, const int32_t* __restrict__ keys,
                                     const int32_t* __restrict__ rank, const int32_t* __restrict__ starts,
                                     int stride, const int32_t* __restrict__ cap, int CS,
-                                    int32_t* __restrict__ ovcur, int32_t* __restrict__ ovlist,
-                                    JfParticles src, JfParticles dst) {
+                                    const int32_t* __restrict__ brow, int32_t* __restrict__ ovcur,
+                                    int32_t* __restrict__ ovlist, JfParticles src, JfParticles dst) {
   const int m = blockIdx.y;
   const JfInst I = inst[m];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -677,7 +750,10 @@ __global__ void sort_scatter_kernel(const JfInst* __restrict__ inst, const int32
   const int32_t rel = starts[(int64_t)m * stride + key] + rk;
   const int64_t d = I.p_off + rel;
   if (key < I.nx * I.ny && rk >= cap[m]) {
-    const int band = min((key / I.nx) / I.band_h, CS - 1);
+    const int row = key / I.nx;
+    const int32_t* br = brow + m * (CS + 1);
+    int band = 0;
+    while (band + 1 < CS && br[band + 1] <= row) ++band;
     ovlist[I.p_off + atomicAdd(ovcur + m * CS + band, 1)] = rel;
   }
   dst.xv[d] = src.xv[g];
@@ -733,12 +809,12 @@ cudaError_t jf_batched_sort(jf_engine* e) {
                                                           e->d_rank, e->d_counts, stride);
   }
   sort_scan_kernel<<<e->M, kScanThreads, 0, e->stream>>>(e->d_inst, e->d_counts, stride, e->d_band,
-                                                         e->d_cap, e->d_ovband, e->d_ovcur, e->cluster,
-                                                         e->cell_cap);
+                                                         e->d_brow, e->d_cap, e->d_ovband, e->d_ovcur,
+                                                         e->cluster, e->cell_cap);
   if (e->max_slots > 0) {
     sort_scatter_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->d_keys, e->d_rank, e->d_counts,
-                                                             stride, e->d_cap, e->cluster, e->d_ovcur,
-                                                             e->d_ovlist, e->p, e->q);
+                                                             stride, e->d_cap, e->cluster, e->d_brow,
+                                                             e->d_ovcur, e->d_ovlist, e->p, e->q);
   }
   e->launches += (e->max_slots > 0) ? 3 : 1;
   err = cudaGetLastError();
@@ -766,6 +842,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.ovlist = e->d_ovlist;
   a.ovband = e->d_ovband;
   a.order = e->d_order;
+  a.brow = e->d_brow;
   a.stride = e->max_cells + 2;
   a.grid = e->d_grid;
   a.err = e->d_err;

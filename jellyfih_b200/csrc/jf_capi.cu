@@ -21,6 +21,7 @@ std::string g_create_err;  // message of the last failed call without a handle
 
 constexpr int kHaloRows = 4;  // batched window rows beyond the band (1 below, 3 above)
 constexpr size_t kMaxSmem = 227 * 1024;
+constexpr size_t kStaticSmem = 1024;  // the chunk kernel's static shared variables, rounded up
 
 int fail(jf_engine* e, int code, const std::string& msg) {
   if (e) e->err = msg;
@@ -306,12 +307,23 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     g_off += (int64_t)d.n_grid * d.n_grid_y;
     e->max_slots = std::max(e->max_slots, d.n_slots);
     e->max_cells = std::max(e->max_cells, d.n_grid * d.n_grid_y);
-    e->win_nodes = std::max(e->win_nodes, (I.band_h + kHaloRows) * d.n_grid);
+    {
+      // the sort may give a band up to 25 % more rows than ceil(ny / CTAs)
+      // when that balances the CTAs' work, as far as shared memory allows
+      const int planes = (cfg->flags & JF_FLAG_AXISYM) ? 6 : 5;
+      const long long fit = (long long)(kMaxSmem - kStaticSmem) / (4LL * planes * d.n_grid) - kHaloRows;
+      long long bc = I.band_h + I.band_h / 4;
+      bc = std::min(bc, fit);
+      bc = std::max<long long>(bc, I.band_h);
+      bc = std::min<long long>(bc, d.n_grid_y);
+      e->inst.back().band_cap = (int32_t)bc;
+    }
+    e->win_nodes = std::max(e->win_nodes, (e->inst.back().band_cap + kHaloRows) * d.n_grid);
   }
   e->total_slots = p_off;
   e->total_nodes = g_off;
   if (p_off >= (int64_t)1 << 31) return bail(JF_ERR_UNSUPPORTED, "more than 2^31 particle slots");
-  if (e->path == JF_PATH_BATCHED && jf_batched_smem_bytes(e) > kMaxSmem)
+  if (e->path == JF_PATH_BATCHED && jf_batched_smem_bytes(e) > kMaxSmem - kStaticSmem)
     return bail(JF_ERR_UNSUPPORTED, "grid band does not fit in shared memory (n_grid * rows too large)");
 
   if (!e->stream) {
@@ -343,6 +355,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
         (err = alloc(&e->d_band, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_cap, e->M)) != cudaSuccess ||
         (err = alloc(&e->d_order, e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_brow, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_path, 4)) != cudaSuccess ||
         (err = alloc(&e->d_time, 1)) != cudaSuccess ||
         (err = cudaMemset(e->d_path, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
@@ -389,7 +402,7 @@ int jf_destroy(jf_engine* e) {
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_rank); cudaFree(e->d_ovlist); cudaFree(e->d_ovband); cudaFree(e->d_ovcur);
-  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_ep); cudaFree(e->d_ep_mat);
+  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_brow); cudaFree(e->d_ep); cudaFree(e->d_ep_mat);
   cudaFree(e->d_ep_stats); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);

@@ -18,7 +18,8 @@
 struct JfInst {
   int32_t nx, ny;       // grid nodes along x and y (n_grid, n_grid_y)
   int32_t dcx, dcy;     // damping band widths n_grid // 20, n_grid_y // 20 (:283-284)
-  int32_t band_h;       // grid rows per CTA band (batched path)
+  int32_t band_h;       // nominal grid rows per CTA band (batched path): ceil(ny / CTAs)
+  int32_t band_cap;     // most rows a band may take when the sort balances bands (batched)
   int32_t n_slots;      // particle slots of this instance
   int64_t p_off;        // first particle slot in the engine arrays
   int64_t g_off;        // first grid node in the engine grid array

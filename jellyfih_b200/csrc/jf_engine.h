@@ -62,6 +62,7 @@ struct jf_engine {
   int32_t* d_band = nullptr;       // batched path: M x (cluster + 1) particle ranges
   int32_t* d_cap = nullptr;        // batched path: per-instance particles per cell lane
   int32_t* d_order = nullptr;      // batched path: cluster -> instance, most live particles first
+  int32_t* d_brow = nullptr;       // batched path: M x (cluster + 1) band row starts
   float* d_ep = nullptr;           // episode staging: pos (2), fiber (2), glow (1) floats per slot
   int32_t* d_ep_mat = nullptr;     // episode staging: material per slot
   double* d_ep_stats = nullptr;    // episode: CoM sums before the run (6 per instance)

@@ -92,7 +92,10 @@ struct ChunkArgs {
 // are reached in the owner CTA's window.
 struct Window {
   float *Gx, *Gy, *Ax, *Ay, *Am, *Ah;
-  int nx, win0, WR, CS;
+  int nx, win0;
+  int WR;  // rows of a plane (the largest band the sort may cut, plus the halo)
+  int VR;  // rows in use: this band's rows plus the halo; rows VR .. WR - 1 stay idle
+  int CS;
   const int* brow;  // shared copy of the instance's band row starts (CS + 1)
 };
 
@@ -106,7 +109,7 @@ __device__ __forceinline__ int owner_row(const Window& w, int j, int o) { return
 
 __device__ __forceinline__ float2 gather_node(const Window& w, cg::cluster_group& cl, int i, int j) {
   const int wr = j - w.win0;
-  if (wr >= 0 && wr < w.WR) {
+  if (wr >= 0 && wr < w.VR) {
     const int n = wr * w.nx + i;
     return make_float2(w.Gx[n], w.Gy[n]);
   }
@@ -125,7 +128,7 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
     const int wr = row - w.win0;
     float *px = w.Ax, *py = w.Ay, *pm = w.Am, *ph = w.Ah;
     int rn = wr * w.nx;
-    if (!(wr >= 0 && wr < w.WR)) {
+    if (!(wr >= 0 && wr < w.VR)) {
       const int o = owner_of(w, row);
       px = cl.map_shared_rank(w.Ax, o);
       py = cl.map_shared_rank(w.Ay, o);
@@ -249,6 +252,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   w.brow = s_brow;
   w.win0 = row0 - kHaloLo;
   w.WR = I.band_cap + kHalo;  // the window holds the largest band the sort may cut
+  w.VR = max(own_hi - row0, 0) + kHalo;
   const int WN = w.WR * nx;
   w.Gx = sm;
   w.Gy = w.Gx + WN;
@@ -324,9 +328,9 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const int n_tasks = n_cell_tasks + n_gen_tasks;
 
   // window rows outside the band (pushed to / pulled from their owners):
-  // row 0 and rows n_own + 1 .. WR - 1
+  // row 0 and rows n_own + 1 .. VR - 1
   const int n_own = max(own_hi - row0, 0);
-  const int n_halo_rows = w.WR - n_own;
+  const int n_halo_rows = w.VR - n_own;  // row 0 and rows n_own + 1 .. n_own + 3
   const bool rows_by_thread = (nth % nx) == 0;  // the grid update can step whole rows
 
   float t = *a.t_dev;
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
             C = C_m[k];
           } else {
             const int wr0 = st.by - w.win0;
-            if (wr0 >= 0 && wr0 + 2 < w.WR) {
+            if (wr0 >= 0 && wr0 + 2 < w.VR) {
               const int wb = wr0 * nx + st.bx;
               jf_g2p_apic(I, st, v, C, [&](int i, int j) {
                 const int n = wb + j * nx + i;

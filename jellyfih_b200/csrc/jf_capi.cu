@@ -22,6 +22,7 @@ std::string g_create_err;  // message of the last failed call without a handle
 constexpr int kHaloRows = 4;  // batched window rows beyond the band (1 below, 3 above)
 constexpr size_t kMaxSmem = 227 * 1024;
 constexpr size_t kStaticSmem = 1024;  // the chunk kernel's static shared variables, rounded up
+constexpr size_t kBandSlackSmem = 128 * 1024;  // window size up to which bands get spare rows
 
 int fail(jf_engine* e, int code, const std::string& msg) {
   if (e) e->err = msg;
@@ -309,9 +310,11 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     e->max_cells = std::max(e->max_cells, d.n_grid * d.n_grid_y);
     {
       // the sort may give a band up to 25 % more rows than ceil(ny / CTAs)
-      // when that balances the CTAs' work, as far as shared memory allows
+      // when that balances the CTAs' work, as long as the window stays within
+      // kBandSlackSmem: shared memory and L1 share an SM's 256 KB, and
+      // particle loads slow down when the window takes most of it
       const int planes = (cfg->flags & JF_FLAG_AXISYM) ? 6 : 5;
-      const long long fit = (long long)(kMaxSmem - kStaticSmem) / (4LL * planes * d.n_grid) - kHaloRows;
+      const long long fit = (long long)kBandSlackSmem / (4LL * planes * d.n_grid) - kHaloRows;
       long long bc = I.band_h + I.band_h / 4;
       bc = std::min(bc, fit);
       bc = std::max<long long>(bc, I.band_h);

@@ -26,7 +26,9 @@ extern "C" {
 #define JF_OK 0
 #define JF_ERR_INVALID 1      /* bad argument, shape or state */
 #define JF_ERR_CUDA 2         /* a CUDA call failed */
-#define JF_ERR_NONFINITE 3    /* a particle state became NaN/Inf */
+#define JF_ERR_NONFINITE 3    /* a particle state became NaN/Inf: returned, after their outputs
+                                 are written, by jf_sync, jf_run_headless and jf_run_episode while
+                                 an instance's flag is set (jf_error_flags / jf_clear_error_flags) */
 #define JF_ERR_UNSUPPORTED 4  /* configuration outside what the chosen path supports */
 
 #define JF_PATH_PLAIN 0       /* one instance per launch sequence (reference structure) */

@@ -519,12 +519,36 @@ int jf_step(jf_engine* e, int64_t n_steps) {
   return step_impl(e, n_steps);
 }
 
+// JF_ERR_NONFINITE when any instance's non-finite flag is set (the caller
+// has synchronised the stream); the message names the instances.
+static int nonfinite_status(jf_engine* e, const std::vector<int32_t>& flags) {
+  std::string which;
+  int n = 0;
+  for (int m = 0; m < e->M; ++m) {
+    if (!flags[m]) continue;
+    if (n < 8) which += (n ? ", " : "") + std::to_string(m);
+    ++n;
+  }
+  if (n == 0) return JF_OK;
+  if (n > 8) which += ", ...";
+  return fail(e, JF_ERR_NONFINITE, std::to_string(n) + " instance(s) with a non-finite particle state: " + which);
+}
+
+static int read_flags_and_sync(jf_engine* e, std::vector<int32_t>& flags) {
+  flags.assign(e->M, 0);
+  JF_CK(cudaMemcpyAsync(flags.data(), e->d_err, sizeof(int32_t) * e->M, cudaMemcpyDeviceToHost, e->stream),
+        "read flags");
+  JF_CK(cudaStreamSynchronize(e->stream), "sync");
+  return JF_OK;
+}
+
 int jf_sync(jf_engine* e) {
   if (check_engine(e)) return JF_ERR_INVALID;
   int rc = set_device(e);
   if (rc) return rc;
-  JF_CK(cudaStreamSynchronize(e->stream), "sync");
-  return JF_OK;
+  std::vector<int32_t> flags;
+  if ((rc = read_flags_and_sync(e, flags))) return rc;
+  return nonfinite_status(e, flags);
 }
 
 int jf_payload_stats(jf_engine* e, double* out) {
@@ -571,7 +595,9 @@ int jf_run_headless(jf_engine* e, int64_t steps, double* out) {
       o[4] = (b[0] < 0.01) ? 0.0 : 1.0;
     }
   }
-  return JF_OK;
+  std::vector<int32_t> flags;
+  if ((rc = read_flags_and_sync(e, flags))) return rc;
+  return nonfinite_status(e, flags);
 }
 
 int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts, const double* contraction,
@@ -663,13 +689,11 @@ int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, cons
           "fitness genes");
     JF_CK(jf_fitness_launch(e, d_rows, e->d_fit_i, e->d_fit_f, mode, d_out), "fitness kernel");
     JF_CK(cudaMemcpyAsync(fitness, d_out, sizeof(double) * M, cudaMemcpyDeviceToHost, e->stream), "fitness read");
-    JF_CK(cudaMemcpyAsync(rows, d_rows, sizeof(double) * 5 * M, cudaMemcpyDeviceToHost, e->stream), "rows read");
-    JF_CK(cudaStreamSynchronize(e->stream), "episode sync");
-  } else {
-    JF_CK(cudaMemcpyAsync(rows, d_rows, sizeof(double) * 5 * M, cudaMemcpyDeviceToHost, e->stream), "rows read");
-    JF_CK(cudaStreamSynchronize(e->stream), "episode sync");
   }
-  return JF_OK;
+  JF_CK(cudaMemcpyAsync(rows, d_rows, sizeof(double) * 5 * M, cudaMemcpyDeviceToHost, e->stream), "rows read");
+  std::vector<int32_t> flags;
+  if ((rc = read_flags_and_sync(e, flags))) return rc;
+  return nonfinite_status(e, flags);
 }
 
 int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss) {

@@ -67,6 +67,7 @@ class Engine:
             raise L.JfError(rc, self._lib.jf_last_error(None).decode())
         self._h = h
         self.dt = dt
+        self.nonfinite_message = ""  # set when a run reported a non-finite particle state
         self.config = dict(path=path, resort_interval=resort_interval, block_threads=block_threads,
                            cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap, axisym=axisym)
 
@@ -74,6 +75,15 @@ class Engine:
     def _check(self, rc):
         if rc != L.JF_OK:
             raise L.JfError(rc, self._lib.jf_last_error(self._h).decode())
+
+    def _check_run(self, rc):
+        """As _check, but a non-finite particle state is recorded, not raised:
+        results are still written and, as in the reference, an exploded
+        instance simply scores as invalid.  error_flags() tells which."""
+        if rc == L.JF_ERR_NONFINITE:
+            self.nonfinite_message = self._lib.jf_last_error(self._h).decode()
+            return
+        self._check(rc)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -157,7 +167,7 @@ class Engine:
         self._check(self._lib.jf_step(self._h, int(n)))
 
     def sync(self) -> None:
-        self._check(self._lib.jf_sync(self._h))
+        self._check_run(self._lib.jf_sync(self._h))
 
     # -- readback ------------------------------------------------------------
     def payload_stats(self) -> np.ndarray:
@@ -178,7 +188,7 @@ class Engine:
 
     def run_headless(self, steps: int) -> np.ndarray:
         out = np.zeros((self.M, 5), np.float64)
-        self._check(self._lib.jf_run_headless(self._h, int(steps), _ptr(out)))
+        self._check_run(self._lib.jf_run_headless(self._h, int(steps), _ptr(out)))
         return out
 
     def fitness(self, results, muscle_counts, contraction=None, mode: str = "efficiency") -> np.ndarray:
@@ -213,9 +223,9 @@ class Engine:
         mus = None if muscle_counts is None else np.ascontiguousarray(muscle_counts, dtype=np.int32).reshape(self.M)
         rows = np.zeros((self.M, 5), np.float64)
         fit = None if mus is None else np.zeros(self.M, np.float64)
-        self._check(self._lib.jf_run_episode(self._h, _ptr(pos), _ptr(mat), _ptr(fib), _ptr(con), _ptr(frq),
-                                             int(steps), _ptr(mus), {"efficiency": 0, "displacement": 1}[mode],
-                                             _ptr(rows), _ptr(fit)))
+        self._check_run(self._lib.jf_run_episode(self._h, _ptr(pos), _ptr(mat), _ptr(fib), _ptr(con), _ptr(frq),
+                                                 int(steps), _ptr(mus), {"efficiency": 0, "displacement": 1}[mode],
+                                                 _ptr(rows), _ptr(fit)))
         return rows, fit
 
     # -- differentiable rollout -----------------------------------------------

@@ -242,6 +242,7 @@ def test_resort_interval_and_drift_beyond_halo():
 
 def test_nonfinite_flag_and_invalid_arguments():
     from jellyfih_b200 import InstanceSpec, JfError
+    from jellyfih_b200 import _lib as L
     e = _engine([InstanceSpec(1000), InstanceSpec(1000)], "batched")
     pos = np.full((1000, 2), 0.5, np.float32)
     pos[:, 0] = np.linspace(0.3, 0.7, 1000)
@@ -254,8 +255,15 @@ def test_nonfinite_flag_and_invalid_arguments():
     e.step(2)
     flags = e.error_flags()
     assert flags[0] == 0 and flags[1] != 0
+    # the synchronising C calls report it (outputs still written); the Python
+    # wrappers record it instead of raising, as exploded instances score invalid
+    assert e._lib.jf_sync(e._h) == L.JF_ERR_NONFINITE
+    assert b"1 instance(s)" in e._lib.jf_last_error(e._h)
+    rows = e.run_headless(1)
+    assert rows.shape == (2, 5) and "non-finite" in e.nonfinite_message
     e.clear_error_flags()
     assert not e.error_flags().any()
+    assert e._lib.jf_sync(e._h) == L.JF_OK
     with pytest.raises(JfError):
         e.load(5, pos, mat)
     with pytest.raises(JfError):

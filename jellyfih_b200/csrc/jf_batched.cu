@@ -1,9 +1,13 @@
 // Batched path: every instance advances in one persistent launch per chunk
-// of substeps.  Instance m is owned by one thread-block cluster of CS CTAs;
-// CTA r of the cluster owns grid rows [r*H, r*H + H) of that instance and
-// keeps them, plus a halo, in shared memory for the whole chunk, so the grid
-// never touches HBM.  Particles are counting-sorted by cell between chunks so
-// that each CTA streams exactly the particles whose stencils fall in its band.
+// of substeps.  Instance m is owned by one thread-block cluster of CS CTAs
+// (clusters take instances in descending live count); CTA r of the cluster
+// owns a band of grid rows of that instance — the bands are cut at each
+// re-sort so that the CTAs carry equal work — and keeps them, plus a halo, in
+// shared memory for the whole chunk, so the grid never touches HBM.
+// Particles are counting-sorted by cell between chunks so that each CTA
+// streams exactly the particles whose stencils fall in its band; a cell keeps
+// at most a per-instance cap of particles for its lane, the rest go to the
+// band's overflow list.
 //
 // One pass over a CTA's particles fuses G2P of substep s-1 with P2G of
 // substep s (mpm_sim.py:312-333 then :168-271), so each substep reads and

@@ -161,6 +161,55 @@ def _oracle_run(pos, mat, fib, c, f, steps, nx=128, ny=128, dh=1.0, act=500.0, p
     return s, O.headless_rows(x0, x1)[0]
 
 
+
+def test_batched_odd_grids_against_oracle():
+    """Grid widths that are not multiples of 32 and do not divide the block
+    (80 x 112 and 96 x 96 nodes): partial 32-cell segments, the generic grid
+    update loop and uneven band heights, against the oracle after 1 and 5
+    substeps."""
+    from jellyfih_b200 import InstanceSpec, tank
+    from oracle import oracle as O
+    shapes = [(80, 112, 112 / 80), (96, 96, 1.0)]
+    gs = tank.uniform_genomes(2, 31)
+    specs, data = [], []
+    for (nx, ny, dh), g in zip(shapes, gs):
+        pos, mat, fib, st = tank.fill_tank(g, 30000, grid_res=nx, domain_height=dh,
+                                           spawn_offset=np.array([0.5, 0.4 * dh]), jitter=0.25, seed=nx)
+        c, f = tank.timing_params(g)
+        specs.append(InstanceSpec(30000, nx, ny, dh))
+        data.append((pos, mat, fib, c, f))
+    e = _engine(specs, "batched", resort_interval=2)
+    for m, (pos, mat, fib, c, f) in enumerate(data):
+        e.load(m, pos, mat, fib)
+    e.set_params(contraction=[d[3] for d in data], freq=[d[4] for d in data])
+    e.time = 0.0
+    states = []
+    for m, (pos, mat, fib, c, f) in enumerate(data):
+        nx, ny, dh = shapes[m]
+        states.append((O.new_state(pos, mat, fib, "f32", nx, ny),
+                       O.Instance(nx=nx, ny=ny, domain_h=dh, contraction=c, freq=f)))
+    t = np.float32(0)
+    done = 0
+    for cp in (1, 5):
+        e.step(cp - done)
+        t_next = t
+        for s, inst in states:
+            t_next = O.run(inst, s, t, cp - done)
+        t = t_next
+        assert e.time == t
+        done = cp
+        tol = FIELD_RTOL if cp == 1 else MULTI_STEP_RTOL
+        for m, (s, inst) in enumerate(states):
+            got = e.read(m)
+            live = data[m][1] >= 0
+            assert_positions_close(got["x"][live], s["x"][live], 4 * cp, f"odd grid {m} x step {cp}")
+            for k in ("v", "C", "F"):
+                assert_norm_close(got[k][live], s[k][live], tol, f"odd grid {m} {k} step {cp}")
+            gv, gm = e.read_grid(m)
+            assert_norm_close(gm, s["grid_m"], tol, f"odd grid {m} grid_m step {cp}")
+    assert not e.error_flags().any()
+    e.close()
+
 @pytest.mark.parametrize("path", PATHS)
 def test_full_tank_1000_steps_against_oracle(path):
     """Config-1 workload: 1 instance, 80K slots, 128^2, 1,000 substeps."""

@@ -91,11 +91,13 @@ struct ChunkArgs {
 };
 
 // Shared-memory window of one CTA: grid rows [win0, win0 + WR) of its
-// instance, planar (updated velocity Gx, Gy; accumulated momentum Ax, Ay,
+// instance: the updated velocity G as float2 pairs (one 64-bit load per node
+// in G2P), then planar accumulators (momentum Ax, Ay,
 // mass Am and, axisymmetric only, the hoop sum Ah).  Rows outside the window
 // are reached in the owner CTA's window.
 struct Window {
-  float *Gx, *Gy, *Ax, *Ay, *Am, *Ah;
+  float2* G;
+  float *Ax, *Ay, *Am, *Ah;
   int nx, win0;
   int WR;  // rows of a plane (the largest band the sort may cut, plus the halo)
   int VR;  // rows in use: this band's rows plus the halo; rows VR .. WR - 1 stay idle
@@ -115,11 +117,11 @@ __device__ __forceinline__ float2 gather_node(const Window& w, cg::cluster_group
   const int wr = j - w.win0;
   if (wr >= 0 && wr < w.VR) {
     const int n = wr * w.nx + i;
-    return make_float2(w.Gx[n], w.Gy[n]);
+    return w.G[n];
   }
   const int o = owner_of(w, j);
   const int n = owner_row(w, j, o) * w.nx + i;
-  return make_float2(cl.map_shared_rank(w.Gx, o)[n], cl.map_shared_rank(w.Gy, o)[n]);
+  return cl.map_shared_rank(w.G, o)[n];
 }
 
 // Scatter of one particle's 9 stencil contributions with atomics, local when
@@ -258,9 +260,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   w.WR = I.band_cap + kHalo;  // the window holds the largest band the sort may cut
   w.VR = max(own_hi - row0, 0) + kHalo;
   const int WN = w.WR * nx;
-  w.Gx = sm;
-  w.Gy = w.Gx + WN;
-  w.Ax = w.Gy + WN;
+  w.G = reinterpret_cast<float2*>(sm);  // 2 * WN floats
+  w.Ax = sm + 2 * WN;
   w.Ay = w.Ax + WN;
   w.Am = w.Ay + WN;
   w.Ah = w.Am + WN;  // a sixth plane exists only in the axisymmetric variant
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
               const int wb = wr0 * nx + st.bx;
               jf_g2p_apic(I, st, v, C, [&](int i, int j) {
                 const int n = wb + j * nx + i;
-                return make_float2(w.Gx[n], w.Gy[n]);
+                return w.G[n];
               });
             } else {
               ++n_gather_generic;
@@ -496,8 +497,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         const int j = w.win0 + wr;
         const float mm = w.Am[n];
         const float2 u = jf_grid_node(I, i, j, w.Ax[n], w.Ay[n], mm, I.axisym ? w.Ah[n] : 0.0f);
-        w.Gx[n] = u.x;
-        w.Gy[n] = u.y;
+        w.G[n] = u;
         if (last) a.grid[I.g_off + (int64_t)j * nx + i] = make_float4(u.x, u.y, mm, 0.0f);
         w.Ax[n] = 0.0f;
         w.Ay[n] = 0.0f;
@@ -525,8 +525,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         const int n = wr * nx + (q - h * nx);
         const int o = owner_of(w, j);
         const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
-        w.Gx[n] = cluster.map_shared_rank(w.Gx, o)[rn];
-        w.Gy[n] = cluster.map_shared_rank(w.Gy, o)[rn];
+        w.G[n] = cluster.map_shared_rank(w.G, o)[rn];
       }
       t = t + a.dt;
       if (tid == 0) {

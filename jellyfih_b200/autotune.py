@@ -12,9 +12,7 @@ from __future__ import annotations
 
 import itertools
 
-import numpy as np
-
-from .engine import Engine, InstanceSpec
+from .engine import Engine
 from ._lib import JfError
 
 

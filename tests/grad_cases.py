@@ -1,6 +1,4 @@
 """Small differentiable-rollout cases shared by the CPU and GPU gradient tests."""
-import numpy as np
-
 from jellyfih_b200 import tank
 
 

@@ -1,7 +1,6 @@
 """The reference gradient (float64 PyTorch autograd restatement, standing in for
 Taichi autodiff) against central finite differences of the FP64 C oracle."""
 import numpy as np
-import pytest
 import torch
 
 import grad_cases

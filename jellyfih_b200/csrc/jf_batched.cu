@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       if (a.do_glow) a.glow[g] = jf_glow(a.glow[g], jp);
       if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
       a.xv[g] = make_float4(x.x, x.y, v.x, v.y);
-      a.C[g] = C;
+      if (!do_p2g) a.C[g] = C;  // stored when no later pass of the chunk recomputes it (see the cell loop)
     }
     if (do_p2g) {
       JfStencil st;
@@ -309,6 +309,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         a.F[g] = F;
         if (mt == 2) a.Jp[g] = jp;
         scatter_particle(w, cluster, I, st, sc);
+      } else if (do_g2p) {
+        a.C[g] = C;  // out of range: the next G2P keeps this C
       }
     }
   };
@@ -422,7 +424,10 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           if (a.do_glow) a.glow[p0 + k] = jf_glow(a.glow[p0 + k], jp);
           if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
           xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
-          C_m[k] = C;
+          // this pass's P2G takes C from registers and the next pass's G2P
+          // recomputes it, so C is stored only by the chunk's last pass and
+          // where the particle leaves the stencil range (P2G below)
+          if (!do_p2g) C_m[k] = C;
         } else {
           C = C_m[k];
         }
@@ -452,6 +457,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
             } else {
               scatter_particle(w, cluster, I, st, sc);
             }
+          } else if (do_g2p) {
+            C_m[k] = C;  // out of range: the next G2P keeps this C
           }
         }
       }

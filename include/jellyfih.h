@@ -178,6 +178,51 @@ int jf_write_particles(jf_engine* e, int32_t m, const float* x, const float* v, 
  * grid_v[nx][ny][2], grid_m[nx][ny]; either may be NULL. */
 int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m);
 
+/* Overwrite grid_v / grid_m of instance m (grid_v.from_numpy, grid_m.from_numpy;
+ * layouts as jf_read_grid).  The next substep recomputes the grid from the
+ * particles, so this feeds the renderer and vorticity calls below. */
+int jf_write_grid(jf_engine* e, int32_t m, const float* grid_v, const float* grid_m);
+
+/* ---- Headless renderer (mpm_sim.py:343-712) --------------------------------
+ * The reference's render kernels into a device frame buffer owned by the
+ * engine (frame_buffer, mpm_sim.py:96); no graphics API is involved.  The
+ * frame holds video_res x video_res RGB floats; instance m draws into tile
+ * (m / grid_side, m % grid_side) of res_sub pixels.  Launches are queued on
+ * the engine's stream; jf_read_frame / jf_read_vorticity synchronise. */
+#define JF_VORT_RDBU 0      /* render_vorticity_rdbu (mpm_sim.py:582-625) */
+#define JF_VORT_HUESHIFT 1  /* render_vorticity_hueshift (mpm_sim.py:628-670) */
+#define JF_VORT_WHITE 2     /* render_vorticity_white (mpm_sim.py:673-711) */
+
+/* (Re)allocate the frame (video_res x video_res) and clear it to 0. */
+int jf_frame_create(jf_engine* e, int32_t video_res);
+/* clear_frame_buffer (value 0, mpm_sim.py:361-364) / clear_frame_buffer_white
+ * (0.98, mpm_sim.py:483-486). */
+int jf_frame_clear(jf_engine* e, float value);
+/* render_frame_abyss (mpm_sim.py:385-481): additive splats of radius
+ * 1.5 * radius, coloured by material; hue / muscle_hue are the per-instance
+ * instance_hue / instance_muscle_hue [n_instances]; water_mode is
+ * water_angle_color (0 ghost, 1 plain, else rainbow).  Uses sim_time and the
+ * per-instance waveform parameters for the muscle colour. */
+int jf_render_abyss(jf_engine* e, int32_t res_sub, int32_t grid_side, float radius, const float* hue,
+                    const float* muscle_hue, int32_t water_mode);
+/* render_flat_pass (mpm_sim.py:489-517): discs of one material in one colour. */
+int jf_render_flat(jf_engine* e, int32_t res_sub, int32_t grid_side, float radius, int32_t material, float r,
+                   float g, float b);
+/* render_vorticity_overlay (mpm_sim.py:520-558): additive curl squares from
+ * the last substep's grid. */
+int jf_render_vorticity_overlay(jf_engine* e, int32_t res_sub, int32_t grid_side, float vort_scale);
+/* compute_vorticity_grid (mpm_sim.py:561-579): tanh(curl * vort_scale) per node. */
+int jf_compute_vorticity(jf_engine* e, float vort_scale);
+/* render_vorticity_rdbu / _hueshift / _white (style JF_VORT_*): blends the
+ * vorticity grid over the frame (white: over a white clear). */
+int jf_render_vorticity(jf_engine* e, int32_t res_sub, int32_t grid_side, float alpha, int32_t style);
+/* tone_map_and_encode (mpm_sim.py:366-383). */
+int jf_tone_map(jf_engine* e);
+/* frame_buffer.to_numpy(): rgb[video_res][video_res][3], row = frame row py. */
+int jf_read_frame(jf_engine* e, float* rgb);
+/* vort_grid of instance m (mpm_sim.py:106): vort[nx][ny]. */
+int jf_read_vorticity(jf_engine* e, int32_t m, float* vort);
+
 /* Per-instance non-finite flags raised by the G2P update since the last
  * clear (out[n_instances]). */
 int jf_error_flags(jf_engine* e, int32_t* out);

@@ -21,6 +21,9 @@ JF_PATH_BATCHED = 1
 JF_FLAG_GLOW = 1
 JF_FLAG_NO_GRAPHS = 2
 JF_FLAG_AXISYM = 4
+JF_VORT_RDBU = 0
+JF_VORT_HUESHIFT = 1
+JF_VORT_WHITE = 2
 
 
 class JfInstanceDesc(ctypes.Structure):
@@ -64,6 +67,19 @@ EXPORTS = {
     "jf_read_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "jf_write_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P]),
     "jf_read_grid": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P]),
+    "jf_write_grid": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P]),
+    "jf_frame_create": (ctypes.c_int, [_E, ctypes.c_int32]),
+    "jf_frame_clear": (ctypes.c_int, [_E, ctypes.c_float]),
+    "jf_render_abyss": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _P, _P,
+                                       ctypes.c_int32]),
+    "jf_render_flat": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_float]),
+    "jf_render_vorticity_overlay": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_int32, ctypes.c_float]),
+    "jf_compute_vorticity": (ctypes.c_int, [_E, ctypes.c_float]),
+    "jf_render_vorticity": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32]),
+    "jf_tone_map": (ctypes.c_int, [_E]),
+    "jf_read_frame": (ctypes.c_int, [_E, _P]),
+    "jf_read_vorticity": (ctypes.c_int, [_E, ctypes.c_int32, _P]),
     "jf_error_flags": (ctypes.c_int, [_E, _P]),
     "jf_clear_error_flags": (ctypes.c_int, [_E]),
     "jf_kernel_launches": (ctypes.c_int64, [_E]),

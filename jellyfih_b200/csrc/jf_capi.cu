@@ -409,6 +409,7 @@ int jf_destroy(jf_engine* e) {
   cudaFree(e->d_ep_stats); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);
+  cudaFree(e->d_frame); cudaFree(e->d_vort); cudaFree(e->d_hue);
   if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
   for (auto& pr : e->step_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto& pr : e->sort_events) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
@@ -892,6 +893,163 @@ int jf_kernel_timing(jf_engine* e, double* step_ms, int64_t* step_launches, doub
   if (step_launches) *step_launches = e->step_launches;
   if (sort_ms) *sort_ms = e->sort_ms;
   if (sort_launches) *sort_launches = e->sort_launches;
+  return JF_OK;
+}
+
+// --- headless renderer (mpm_sim.py:343-712) -----------------------------------
+
+static int need_frame(jf_engine* e) {
+  if (!e->d_frame) return fail(e, JF_ERR_INVALID, "no frame buffer: call jf_frame_create first");
+  return JF_OK;
+}
+
+static int check_tiles(jf_engine* e, int32_t res_sub, int32_t grid_side) {
+  if (res_sub <= 0 || grid_side <= 0) return fail(e, JF_ERR_INVALID, "res_sub and grid_side must be > 0");
+  return JF_OK;
+}
+
+static int need_vort(jf_engine* e) {
+  if (e->d_vort) return JF_OK;
+  JF_CK(alloc(&e->d_vort, (size_t)e->total_nodes), "cudaMalloc vorticity");
+  JF_CK(cudaMemsetAsync(e->d_vort, 0, sizeof(float) * std::max<int64_t>(e->total_nodes, 1), e->stream),
+        "clear vorticity");
+  return JF_OK;
+}
+
+int jf_frame_create(jf_engine* e, int32_t video_res) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (video_res <= 0 || video_res > 16384) return fail(e, JF_ERR_INVALID, "video_res must be in 1 .. 16384");
+  int rc = set_device(e);
+  if (rc) return rc;
+  if (e->frame_res != video_res) {
+    JF_CK(cudaStreamSynchronize(e->stream), "frame sync");
+    cudaFree(e->d_frame);
+    e->d_frame = nullptr;
+    e->frame_res = 0;
+    JF_CK(alloc(&e->d_frame, (size_t)video_res * video_res), "cudaMalloc frame");
+    e->frame_res = video_res;
+  }
+  JF_CK(cudaMemsetAsync(e->d_frame, 0, sizeof(float4) * (size_t)video_res * video_res, e->stream), "clear frame");
+  return JF_OK;
+}
+
+int jf_frame_clear(jf_engine* e, float value) {
+  if (check_engine(e) || need_frame(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(jf_frame_clear_launch(e, value), "clear frame");
+  return JF_OK;
+}
+
+int jf_render_abyss(jf_engine* e, int32_t res_sub, int32_t grid_side, float radius, const float* hue,
+                    const float* muscle_hue, int32_t water_mode) {
+  if (check_engine(e) || need_frame(e) || check_tiles(e, res_sub, grid_side)) return JF_ERR_INVALID;
+  if (!hue || !muscle_hue) return fail(e, JF_ERR_INVALID, "hue and muscle_hue are required");
+  int rc = set_device(e);
+  if (rc) return rc;
+  if ((rc = upload_params(e))) return rc;
+  if (!e->d_hue) JF_CK(alloc(&e->d_hue, (size_t)e->M), "cudaMalloc hues");
+  std::vector<float2> h(e->M);
+  for (int m = 0; m < e->M; ++m) h[m] = make_float2(hue[m], muscle_hue[m]);
+  JF_CK(cudaMemcpyAsync(e->d_hue, h.data(), sizeof(float2) * e->M, cudaMemcpyHostToDevice, e->stream), "upload hues");
+  JF_CK(jf_render_abyss_launch(e, res_sub, grid_side, radius, water_mode), "render abyss");
+  // the hues' host copy must outlive the copy
+  JF_CK(cudaStreamSynchronize(e->stream), "render abyss sync");
+  return JF_OK;
+}
+
+int jf_render_flat(jf_engine* e, int32_t res_sub, int32_t grid_side, float radius, int32_t material, float r,
+                   float g, float b) {
+  if (check_engine(e) || need_frame(e) || check_tiles(e, res_sub, grid_side)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(jf_render_flat_launch(e, res_sub, grid_side, radius, material, r, g, b), "render flat pass");
+  return JF_OK;
+}
+
+int jf_render_vorticity_overlay(jf_engine* e, int32_t res_sub, int32_t grid_side, float vort_scale) {
+  if (check_engine(e) || need_frame(e) || check_tiles(e, res_sub, grid_side)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(jf_render_overlay_launch(e, res_sub, grid_side, vort_scale), "render vorticity overlay");
+  return JF_OK;
+}
+
+int jf_compute_vorticity(jf_engine* e, float vort_scale) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc || (rc = need_vort(e))) return rc;
+  JF_CK(jf_vorticity_launch(e, vort_scale), "compute vorticity");
+  return JF_OK;
+}
+
+int jf_render_vorticity(jf_engine* e, int32_t res_sub, int32_t grid_side, float alpha, int32_t style) {
+  if (check_engine(e) || need_frame(e) || check_tiles(e, res_sub, grid_side)) return JF_ERR_INVALID;
+  if (style < JF_VORT_RDBU || style > JF_VORT_WHITE) return fail(e, JF_ERR_INVALID, "unknown vorticity style");
+  int rc = set_device(e);
+  if (rc || (rc = need_vort(e))) return rc;
+  JF_CK(jf_render_vort_launch(e, res_sub, grid_side, alpha, style), "render vorticity");
+  return JF_OK;
+}
+
+int jf_tone_map(jf_engine* e) {
+  if (check_engine(e) || need_frame(e)) return JF_ERR_INVALID;
+  int rc = set_device(e);
+  if (rc) return rc;
+  JF_CK(jf_tone_map_launch(e), "tone map");
+  return JF_OK;
+}
+
+int jf_read_frame(jf_engine* e, float* rgb) {
+  if (check_engine(e) || need_frame(e)) return JF_ERR_INVALID;
+  if (!rgb) return fail(e, JF_ERR_INVALID, "rgb is NULL");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const size_t n = (size_t)e->frame_res * e->frame_res;
+  std::vector<float4> f(n);
+  JF_CK(cudaMemcpyAsync(f.data(), e->d_frame, sizeof(float4) * n, cudaMemcpyDeviceToHost, e->stream), "read frame");
+  JF_CK(cudaStreamSynchronize(e->stream), "read frame sync");
+  for (size_t k = 0; k < n; ++k) {
+    rgb[3 * k] = f[k].x;
+    rgb[3 * k + 1] = f[k].y;
+    rgb[3 * k + 2] = f[k].z;
+  }
+  return JF_OK;
+}
+
+int jf_read_vorticity(jf_engine* e, int32_t m, float* vort) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  if (!vort) return fail(e, JF_ERR_INVALID, "vort is NULL");
+  int rc = set_device(e);
+  if (rc || (rc = need_vort(e))) return rc;
+  const JfInst& I = e->inst[m];
+  std::vector<float> g((size_t)I.nx * I.ny);
+  JF_CK(cudaMemcpyAsync(g.data(), e->d_vort + I.g_off, sizeof(float) * g.size(), cudaMemcpyDeviceToHost, e->stream),
+        "read vorticity");
+  JF_CK(cudaStreamSynchronize(e->stream), "read vorticity sync");
+  for (int j = 0; j < I.ny; ++j)
+    for (int i = 0; i < I.nx; ++i) vort[(size_t)i * I.ny + j] = g[(size_t)j * I.nx + i];
+  return JF_OK;
+}
+
+int jf_write_grid(jf_engine* e, int32_t m, const float* grid_v, const float* grid_m) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  if (!grid_v || !grid_m) return fail(e, JF_ERR_INVALID, "grid_v and grid_m are required");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const JfInst& I = e->inst[m];
+  std::vector<float4> g((size_t)I.nx * I.ny);
+  for (int j = 0; j < I.ny; ++j) {
+    for (int i = 0; i < I.nx; ++i) {
+      const size_t r = (size_t)i * I.ny + j;  // reference layout [nx][ny]
+      g[(size_t)j * I.nx + i] = make_float4(grid_v[2 * r], grid_v[2 * r + 1], grid_m[r], 0.0f);
+    }
+  }
+  JF_CK(cudaMemcpyAsync(e->d_grid + I.g_off, g.data(), sizeof(float4) * g.size(), cudaMemcpyHostToDevice, e->stream),
+        "write grid");
+  JF_CK(cudaStreamSynchronize(e->stream), "write grid sync");
   return JF_OK;
 }
 

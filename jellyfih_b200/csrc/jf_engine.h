@@ -92,6 +92,11 @@ struct jf_engine {
   std::string err;
 
   JfGrad* grad = nullptr;          // differentiable rollout buffers (jf_grad.cu)
+  // headless renderer (jf_render.cu)
+  float4* d_frame = nullptr;       // frame_res^2 pixels (r, g, b, unused), row py = frame row
+  int32_t frame_res = 0;
+  float* d_vort = nullptr;         // tanh-mapped curl per grid node (node layout of d_grid)
+  float2* d_hue = nullptr;         // per instance (jelly hue, muscle hue) of the last abyss pass
 
   // optional device timing of step and sort kernels
   bool timing = false;
@@ -151,3 +156,12 @@ cudaError_t jf_stats_launch(jf_engine* e);
 cudaError_t jf_load_launch(jf_engine* e, int m, int32_t n);
 // Copies instance m's glow into slot order at d_stage + 4 * max_slots.
 cudaError_t jf_glow_to_slot_order(jf_engine* e, int m);
+// Headless renderer (jf_render.cu): the reference's render kernels on e->d_frame.
+cudaError_t jf_frame_clear_launch(jf_engine* e, float value);
+cudaError_t jf_render_abyss_launch(jf_engine* e, int res_sub, int grid_side, float radius, int water_mode);
+cudaError_t jf_render_flat_launch(jf_engine* e, int res_sub, int grid_side, float radius, int material, float r,
+                                  float g, float b);
+cudaError_t jf_render_overlay_launch(jf_engine* e, int res_sub, int grid_side, float scale);
+cudaError_t jf_vorticity_launch(jf_engine* e, float scale);
+cudaError_t jf_render_vort_launch(jf_engine* e, int res_sub, int grid_side, float alpha, int style);
+cudaError_t jf_tone_map_launch(jf_engine* e);

@@ -272,6 +272,60 @@ class Engine:
         self._check(self._lib.jf_read_grid(self._h, m, _ptr(gv), _ptr(gm)))
         return gv, gm
 
+    def write_grid(self, m: int, grid_v, grid_m) -> None:
+        """grid_v (nx, ny, 2) / grid_m (nx, ny) of instance m (from_numpy)."""
+        s = self.instances[m]
+        gv = _f32(grid_v, (s.n_grid, s.n_grid_y, 2))
+        gm = _f32(grid_m, (s.n_grid, s.n_grid_y))
+        self._check(self._lib.jf_write_grid(self._h, m, _ptr(gv), _ptr(gm)))
+
+    # --- headless renderer (mpm_sim.py:343-712) --------------------------------
+    def frame_create(self, video_res: int) -> None:
+        """Allocate (or resize) the device frame buffer and clear it to 0."""
+        self._check(self._lib.jf_frame_create(self._h, int(video_res)))
+        self.frame_res = int(video_res)
+
+    def frame_clear(self, value: float = 0.0) -> None:
+        self._check(self._lib.jf_frame_clear(self._h, float(value)))
+
+    def render_abyss(self, res_sub, grid_side, radius, hue, muscle_hue, water_mode=0) -> None:
+        h = _f32(hue, (self.M,))
+        mh = _f32(muscle_hue, (self.M,))
+        self._check(self._lib.jf_render_abyss(self._h, int(res_sub), int(grid_side), float(radius), _ptr(h),
+                                              _ptr(mh), int(water_mode)))
+
+    def render_flat(self, res_sub, grid_side, radius, material, r, g, b) -> None:
+        self._check(self._lib.jf_render_flat(self._h, int(res_sub), int(grid_side), float(radius), int(material),
+                                             float(r), float(g), float(b)))
+
+    def render_vorticity_overlay(self, res_sub, grid_side, vort_scale) -> None:
+        self._check(self._lib.jf_render_vorticity_overlay(self._h, int(res_sub), int(grid_side),
+                                                          float(vort_scale)))
+
+    def compute_vorticity(self, vort_scale) -> None:
+        self._check(self._lib.jf_compute_vorticity(self._h, float(vort_scale)))
+
+    def render_vorticity(self, res_sub, grid_side, alpha, style) -> None:
+        """style: L.JF_VORT_RDBU, JF_VORT_HUESHIFT or JF_VORT_WHITE."""
+        self._check(self._lib.jf_render_vorticity(self._h, int(res_sub), int(grid_side), float(alpha),
+                                                  int(style)))
+
+    def tone_map(self) -> None:
+        self._check(self._lib.jf_tone_map(self._h))
+
+    def read_frame(self) -> np.ndarray:
+        """(video_res, video_res, 3) float32, frame_buffer.to_numpy() layout."""
+        res = getattr(self, "frame_res", 0)
+        out = np.zeros((max(res, 1), max(res, 1), 3), np.float32)
+        self._check(self._lib.jf_read_frame(self._h, _ptr(out)))
+        return out
+
+    def read_vorticity(self, m: int) -> np.ndarray:
+        s = self.instances[m]
+        out = np.zeros((s.n_grid, s.n_grid_y), np.float32)
+        self._check(self._lib.jf_read_vorticity(self._h, m, _ptr(out)))
+        return out
+
     def error_flags(self) -> np.ndarray:
         out = np.zeros(self.M, np.int32)
         self._check(self._lib.jf_error_flags(self._h, _ptr(out)))

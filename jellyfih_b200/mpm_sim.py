@@ -16,7 +16,12 @@ Engine selection (not in the reference): JELLY_B200_PATH = batched (default)
 or plain; JELLY_B200_GLOW = 1 keeps the render-only visual_glow updated.
 JELLY_AXISYM=1 selects the axisymmetric (r, z) substep, as in the reference;
 its r_ref (the load radius) lives inside the engine and is not exposed as a
-field.  The renderer kernels (mpm_sim.py:343-712) are not provided.
+field.  The renderer (mpm_sim.py:343-712) runs as CUDA kernels into a device
+frame buffer: ``clear_frame_buffer``, ``clear_frame_buffer_white``,
+``render_frame_abyss``, ``render_flat_pass``, ``render_vorticity_overlay``,
+``compute_vorticity_grid``, ``render_vorticity_rdbu`` / ``_hueshift`` /
+``_white``, ``tone_map_and_encode``; ``frame_buffer`` and ``vort_grid`` read
+back with ``to_numpy()``.
 """
 from __future__ import annotations
 
@@ -289,11 +294,94 @@ def run_batch_headless(steps):
     return _engine.run_headless(int(steps))
 
 
-def _render_unavailable(*_a, **_k):
-    raise NotImplementedError("the renderer (mpm_sim.py:343-712) is not part of this engine")
+# --- headless renderer (mpm_sim.py:343-712) ----------------------------------
+# The frame lives on the GPU (allocated at the first render call, video_res x
+# video_res); frame_buffer.to_numpy() reads it back.  hsv2rgb is a device
+# function of the kernels, not a Python-scope call, in the reference too.
+def _frame():
+    if getattr(_engine, "frame_res", 0) != video_res:
+        _engine.frame_create(video_res)
 
 
-clear_frame_buffer = clear_frame_buffer_white = tone_map_and_encode = _render_unavailable
-render_frame_abyss = render_flat_pass = render_vorticity_overlay = _render_unavailable
-compute_vorticity_grid = render_vorticity_rdbu = render_vorticity_hueshift = _render_unavailable
-render_vorticity_white = _render_unavailable
+class _FrameBuffer:
+    """frame_buffer (mpm_sim.py:96): (video_res, video_res, 3) float32."""
+
+    @property
+    def shape(self):
+        return (video_res, video_res, 3)
+
+    def to_numpy(self):
+        _frame()
+        return _engine.read_frame()
+
+
+class _VortGrid:
+    """vort_grid (mpm_sim.py:106): (n_instances, n_grid, n_grid_y) float32."""
+    shape = (n_instances, n_grid, n_grid_y)
+
+    def to_numpy(self):
+        return np.stack([_engine.read_vorticity(m) for m in range(n_instances)])
+
+
+frame_buffer = _FrameBuffer()
+vort_grid = _VortGrid()
+
+
+def clear_frame_buffer():
+    """mpm_sim.py:361-364."""
+    _frame()
+    _engine.frame_clear(0.0)
+
+
+def clear_frame_buffer_white():
+    """mpm_sim.py:483-486."""
+    _frame()
+    _engine.frame_clear(0.98)
+
+
+def tone_map_and_encode():
+    """mpm_sim.py:366-383."""
+    _frame()
+    _engine.tone_map()
+
+
+def render_frame_abyss(p_res_sub, p_grid_side, radius):
+    """mpm_sim.py:385-481."""
+    _frame()
+    _engine.render_abyss(p_res_sub, p_grid_side, radius, instance_hue.to_numpy(),
+                         instance_muscle_hue.to_numpy(), int(water_angle_color[None]))
+
+
+def render_flat_pass(p_res_sub, p_grid_side, radius, target_mat, cr, cg, cb):
+    """mpm_sim.py:489-517."""
+    _frame()
+    _engine.render_flat(p_res_sub, p_grid_side, radius, target_mat, cr, cg, cb)
+
+
+def render_vorticity_overlay(p_res_sub, p_grid_side, vort_scale):
+    """mpm_sim.py:520-558."""
+    _frame()
+    _engine.render_vorticity_overlay(p_res_sub, p_grid_side, vort_scale)
+
+
+def compute_vorticity_grid(vort_scale):
+    """mpm_sim.py:561-579."""
+    _engine.compute_vorticity(vort_scale)
+
+
+def render_vorticity_rdbu(p_res_sub, p_grid_side, alpha_max):
+    """mpm_sim.py:582-625."""
+    _frame()
+    _engine.render_vorticity(p_res_sub, p_grid_side, alpha_max, 0)
+
+
+def render_vorticity_hueshift(p_res_sub, p_grid_side, strength):
+    """mpm_sim.py:628-670."""
+    _frame()
+    _engine.render_vorticity(p_res_sub, p_grid_side, strength, 1)
+
+
+def render_vorticity_white(p_res_sub, p_grid_side, alpha_max):
+    """mpm_sim.py:673-711."""
+    _frame()
+    _engine.render_vorticity(p_res_sub, p_grid_side, alpha_max, 2)

@@ -1,4 +1,5 @@
-"""ctypes front end of the CPU oracle (oracle/mpm_oracle.c).
+"""ctypes front end of the CPU oracle (oracle/mpm_oracle.c: the substep;
+oracle/render_oracle.c: the headless renderer).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, always as the checker or the timed CPU baseline,
@@ -52,8 +53,9 @@ class Instance:
 
 def build(force: bool = False) -> str:
     """Compile liboracle_mpm.so with the committed Makefile."""
-    if force or not os.path.exists(_LIB_PATH) or (
-            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "mpm_oracle.c"))):
+    if force or not os.path.exists(_LIB_PATH) or any(
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, f))
+            for f in ("mpm_oracle.c", "render_oracle.c")):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
@@ -78,6 +80,14 @@ def lib():
                 ctypes.POINTER(OracleInst), ctypes.c_float if sfx == "f32" else ctypes.c_double]
             getattr(L, f"oracle_activation_{sfx}").restype = (
                 ctypes.c_float if sfx == "f32" else ctypes.c_double)
+        I32, F32, RI = ctypes.c_int32, ctypes.c_float, ctypes.POINTER(RoInst)
+        L.ro_clear.argtypes = [P, I32, F32]
+        L.ro_tone_map.argtypes = [P, I32]
+        L.ro_abyss.argtypes = [P, I32, I32, RI, P, P, P, P, F32, I32, I32, F32, I32]
+        L.ro_flat.argtypes = [P, I32, I32, RI, P, P, I32, I32, F32, I32, F32, F32, F32]
+        L.ro_vort_overlay.argtypes = [P, I32, I32, RI, P, P, I32, I32, F32]
+        L.ro_vort_grid.argtypes = [P, I32, RI, P, P, F32]
+        L.ro_vort_blend.argtypes = [P, I32, I32, RI, P, I32, I32, F32, I32]
         _lib = L
     return _lib
 
@@ -249,3 +259,86 @@ def svd2(A):
 def activation(inst: Instance, t, precision="f32"):
     ci = inst.c()
     return getattr(lib(), f"oracle_activation_{precision}")(ctypes.byref(ci), t)
+
+
+# --- renderer (render_oracle.c, mpm_sim.py:343-712) ----------------------------
+class RoInst(ctypes.Structure):
+    _fields_ = [("n_slots", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+                ("domain_h", ctypes.c_float), ("freq", ctypes.c_float), ("contraction", ctypes.c_float),
+                ("hue", ctypes.c_float), ("muscle_hue", ctypes.c_float)]
+
+
+class RenderScene:
+    """What the renderer reads, for every instance: particle x, v, material,
+    Jp (slot order), grid_v (nx, ny, 2) and grid_m (nx, ny) of the last
+    substep, grid shape, domain height, waveform parameters, hues, sim_time."""
+
+    def __init__(self, x, v, material, Jp, grid_v, grid_m, domain_h, freq, contraction, hue,
+                 muscle_hue, t):
+        M = len(x)
+        self.M = M
+        self.x = np.ascontiguousarray(np.concatenate(x), np.float32)
+        self.v = np.ascontiguousarray(np.concatenate(v), np.float32)
+        self.mat = np.ascontiguousarray(np.concatenate(material), np.int32)
+        self.Jp = np.ascontiguousarray(np.concatenate(Jp), np.float32)
+        self.gv = np.ascontiguousarray(np.concatenate([g.reshape(-1) for g in grid_v]), np.float32)
+        self.gm = np.ascontiguousarray(np.concatenate([g.reshape(-1) for g in grid_m]), np.float32)
+        self.shapes = [g.shape for g in grid_m]
+        self.t = float(np.float32(t))
+        arr = (RoInst * M)()
+        for m in range(M):
+            arr[m] = RoInst(len(material[m]), grid_m[m].shape[0], grid_m[m].shape[1], float(domain_h[m]),
+                            float(freq[m]), float(contraction[m]), float(hue[m]), float(muscle_hue[m]))
+        self.inst = arr
+
+
+def new_frame(res, value=0.0):
+    return np.full((res, res, 3), value, np.float32)
+
+
+def _fp(a):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def render_clear(fb, value):
+    lib().ro_clear(_fp(fb), fb.shape[0], float(value))
+
+
+def render_tone_map(fb):
+    lib().ro_tone_map(_fp(fb), fb.shape[0])
+
+
+def render_abyss(fb, sc: RenderScene, res_sub, grid_side, radius, water_mode):
+    lib().ro_abyss(_fp(fb), fb.shape[0], sc.M, sc.inst, sc.x.ctypes.data, sc.v.ctypes.data,
+                   sc.mat.ctypes.data, sc.Jp.ctypes.data, sc.t, int(res_sub), int(grid_side),
+                   float(radius), int(water_mode))
+
+
+def render_flat(fb, sc: RenderScene, res_sub, grid_side, radius, target, r, g, b):
+    lib().ro_flat(_fp(fb), fb.shape[0], sc.M, sc.inst, sc.x.ctypes.data, sc.mat.ctypes.data,
+                  int(res_sub), int(grid_side), float(radius), int(target), float(r), float(g), float(b))
+
+
+def render_vorticity_overlay(fb, sc: RenderScene, res_sub, grid_side, scale):
+    lib().ro_vort_overlay(_fp(fb), fb.shape[0], sc.M, sc.inst, sc.gv.ctypes.data, sc.gm.ctypes.data,
+                          int(res_sub), int(grid_side), float(scale))
+
+
+def vorticity_grid(sc: RenderScene, scale):
+    """tanh-mapped curl per node, one (nx, ny) array per instance."""
+    out = np.zeros(sc.gm.shape, np.float32)
+    lib().ro_vort_grid(_fp(out), sc.M, sc.inst, sc.gv.ctypes.data, sc.gm.ctypes.data, float(scale))
+    res, o = [], 0
+    for shp in sc.shapes:
+        n = shp[0] * shp[1]
+        res.append(out[o:o + n].reshape(shp))
+        o += n
+    return res
+
+
+def render_vorticity(fb, sc: RenderScene, vort, res_sub, grid_side, alpha, style):
+    """style 0 rdbu, 1 hueshift, 2 white (over a cleared white frame)."""
+    flat = np.ascontiguousarray(np.concatenate([a.reshape(-1) for a in vort]), np.float32)
+    lib().ro_vort_blend(_fp(fb), fb.shape[0], sc.M, sc.inst, flat.ctypes.data, int(res_sub),
+                        int(grid_side), float(alpha), int(style))

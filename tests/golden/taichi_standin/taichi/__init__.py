@@ -20,7 +20,10 @@ module imports and its @ti.kernel functions execute as plain Python:
   decomposition A = R S with R = [[c,-s],[s,c]] from (A00+A11, A10-A01), then
   one Jacobi rotation of S (skipped when |S01| < 1e-5), singular values sorted
   descending with the matching V, U = R V.
-* ``ti.cos`` is evaluated in double and rounded to f32 once.
+* ``ti.cos``, ``ti.tanh`` and ``ti.atan2`` are evaluated in double and
+  rounded to f32 once; ``float(i)`` of a loop index is a Python float (the
+  renderer's pixel mappings stay exact in both, since their operands are small
+  integers over powers of two).
 
 Nothing here is used by the product; it exists so that tests/golden/
 make_golden.py can record the reference's outputs.
@@ -82,6 +85,9 @@ class _I32:
 
     def __int__(self):
         return self.v
+
+    def __float__(self):
+        return float(self.v)
 
     def __hash__(self):
         return hash(self.v)
@@ -337,6 +343,10 @@ def tanh(a):
 
 def atan(a):
     return np.float32(_pymath.atan(float(a)))
+
+
+def atan2(y, x):
+    return np.float32(_pymath.atan2(float(y), float(x)))
 
 
 def pow(a, b):  # noqa: A001 - mirrors ti.pow

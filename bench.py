@@ -17,7 +17,9 @@ dominant kernel (the batched chunk kernel) at 100 algorithmic bytes per live
 particle-substep (x, v, C, F read and written, material read) against the
 measured HBM copy bandwidth.  ``cpu_baseline`` times the CPU oracle (a
 restatement of the reference's substep) on the host cores.  ``plain`` times
-the plain per-instance launch path on the same inputs.
+the plain per-instance launch path on the same inputs.  ``render`` times the
+headless renderer (a 1024^2 viewer frame of every particle) on the final
+state, beside the CPU oracle rendering the same frame.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -55,6 +57,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the 256 x 64^2 gradient-refinement leg")
+    ap.add_argument("--no-render", action="store_true", help="skip the headless-renderer leg")
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiable leg (8 of the workload's instances) and print it")
     return ap.parse_args()
@@ -319,6 +322,77 @@ def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
             "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast}
 
 
+def render_leg(engine, stream, M, cpu, frames=20, res=1024):
+    """One headless frame per step of the reference's viewer pipeline
+    (run_population.py:60-65 plus the vorticity views): clear, abyss splats of
+    every particle (rainbow water, radius 1.5), vorticity overlay, tone map,
+    vorticity grid, RdBu blend, on the engine's current state; device time
+    with CUDA events.  ``cpu`` adds the CPU oracle rendering the same frame
+    (one thread) and the frame read-back."""
+    import torch
+    from oracle import oracle as O
+    gs = int(np.ceil(np.sqrt(M)))
+    rs = res // gs
+    hue = np.full(M, 0.55, np.float32)
+    mhue = np.full(M, 0.70, np.float32)
+    engine.frame_create(res)
+
+    def frame():
+        engine.frame_clear(0.0)
+        engine.render_abyss(rs, gs, 1.5, hue, mhue, 2)
+        engine.render_vorticity_overlay(rs, gs, 0.001)
+        engine.tone_map()
+        engine.compute_vorticity(0.003)
+        engine.render_vorticity(rs, gs, 0.6, 0)
+
+    for _ in range(3):
+        frame()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    l0 = engine.kernel_launches
+    ev[0].record(stream)
+    for _ in range(frames):
+        frame()
+    ev[1].record(stream)
+    launches = engine.kernel_launches - l0
+    for _ in range(frames):
+        engine.render_abyss(rs, gs, 1.5, hue, mhue, 2)
+    ev[2].record(stream)
+    ev[2].synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / frames
+    abyss_ms = ev[1].elapsed_time(ev[2]) / frames
+    live = sum(int((engine.read(m)["material"] >= 0).sum()) for m in range(M))
+    out = {"ms_per_frame": ms, "frames_per_s": 1e3 / ms, "abyss_ms": abyss_ms,
+           "splat_particles_per_s": live / (abyss_ms / 1e3), "video_res": res, "grid_side": gs,
+           "res_sub": rs, "particles": live, "kernels_per_frame": launches / frames,
+           "pipeline": "clear, abyss (rainbow water, radius 1.5), vorticity overlay, tone map, vorticity grid, rdbu"}
+    frame()  # one clean frame (the abyss-only passes above accumulated)
+    engine.sync()
+    t0 = time.perf_counter()
+    img = engine.read_frame()
+    out["read_frame_ms"] = (time.perf_counter() - t0) * 1e3
+    if cpu:
+        st = [engine.read(m) for m in range(M)]
+        grids = [engine.read_grid(m) for m in range(M)]
+        prm = engine.get_params()
+        sc = O.RenderScene([s["x"] for s in st], [s["v"] for s in st], [s["material"] for s in st],
+                           [s["Jp"] for s in st], [g[0] for g in grids], [g[1] for g in grids], [1.0] * M,
+                           prm["freq"], prm["contraction"], hue, mhue, engine.time)
+        fb = O.new_frame(res)
+        t0 = time.perf_counter()
+        O.render_clear(fb, 0.0)
+        O.render_abyss(fb, sc, rs, gs, 1.5, 2)
+        O.render_vorticity_overlay(fb, sc, rs, gs, 0.001)
+        O.render_tone_map(fb)
+        vort = O.vorticity_grid(sc, 0.003)
+        O.render_vorticity(fb, sc, vort, rs, gs, 0.6, 0)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"ms_per_frame": cpu_s * 1e3, "cores": 1, "kind": "port",
+                               "sample": "one frame of the same pipeline on the same state"}
+        out["gpu_over_cpu"] = cpu_s * 1e3 / ms
+        out["max_abs_diff_vs_oracle"] = float(np.max(np.abs(img - fb)))
+    return out
+
+
 def run_reference(args):
     """--impl reference: the CPU oracle (the reference's substep restated; Taichi
     is not installed) on the host cores, rank 0 only."""
@@ -509,6 +583,9 @@ def run_ours(args):
 
         if not args.no_uneven:
             extras["uneven"] = uneven_leg(local, stream)
+
+        if not args.no_render:
+            extras["render"] = render_leg(engine, stream, M, cpu=(rank == 0 and world == 1))
 
         if rank == 0 and world == 1:
             extras["cpu_baseline"] = cpu_baseline(inputs)

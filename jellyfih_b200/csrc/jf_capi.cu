@@ -951,10 +951,9 @@ int jf_render_abyss(jf_engine* e, int32_t res_sub, int32_t grid_side, float radi
   if (!e->d_hue) JF_CK(alloc(&e->d_hue, (size_t)e->M), "cudaMalloc hues");
   std::vector<float2> h(e->M);
   for (int m = 0; m < e->M; ++m) h[m] = make_float2(hue[m], muscle_hue[m]);
+  // a copy from pageable memory has staged the source when it returns
   JF_CK(cudaMemcpyAsync(e->d_hue, h.data(), sizeof(float2) * e->M, cudaMemcpyHostToDevice, e->stream), "upload hues");
   JF_CK(jf_render_abyss_launch(e, res_sub, grid_side, radius, water_mode), "render abyss");
-  // the hues' host copy must outlive the copy
-  JF_CK(cudaStreamSynchronize(e->stream), "render abyss sync");
   return JF_OK;
 }
 

@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the 256 x 64^2 gradient-refinement leg")
     ap.add_argument("--no-render", action="store_true", help="skip the headless-renderer leg")
+    ap.add_argument("--render-only", action="store_true",
+                    help="run only the renderer leg on the workload after --substeps substeps and print it")
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiable leg (8 of the workload's instances) and print it")
     return ap.parse_args()
@@ -625,12 +627,31 @@ def run_grad_only(args):
     return 0
 
 
+def run_render_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    from jellyfih_b200 import Engine, InstanceSpec
+    inputs = make_inputs(args.instances, args.slots, 1000)
+    engine = Engine([InstanceSpec(args.slots)] * args.instances, path="batched", device=0)
+    stream = torch.cuda.Stream()
+    engine.set_stream(stream)
+    load_all(engine, inputs)
+    engine.step(args.substeps)
+    engine.sync()
+    out = {"render": render_leg(engine, stream, args.instances, cpu=True), "substeps_before": args.substeps}
+    engine.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.grad_only:
         return run_grad_only(args)
+    if args.render_only:
+        return run_render_only(args)
     return run_ours(args)
 
 

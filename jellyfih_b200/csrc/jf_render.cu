@@ -69,8 +69,9 @@ __global__ void __launch_bounds__(kThreads) abyss_kernel(const JfInst* __restric
   if (k >= I.n_slots) return;
   const int64_t g = I.p_off + k;
   const int mt = mat[g];
+  if (mt < 0) return;  // dead slots skip the position load
   const float4 a = xv[g];
-  if (mt < 0 || a.x < 0.0f) return;
+  if (a.x < 0.0f) return;
   const float dh = (float)I.domain_h;
   const int row = m / grid_side, col = m % grid_side;
   const float vel = sqrtf(fadd(fmul(a.z, a.z), fmul(a.w, a.w)));

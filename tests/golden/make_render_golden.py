@@ -130,6 +130,10 @@ def _run_case(case, reference):
     contraction = rng.uniform(0.2, 0.4, M).astype(np.float32)
     hue = rng.uniform(0.0, 1.0, M).astype(np.float32)
     mhue = ((hue + 0.15) % 1.0).astype(np.float32)
+    if M == 3:
+        # hues outside [0, 1) reach hsv2rgb's int() truncation and Python-style %
+        hue = np.array([-0.3, 1.25, 0.5], np.float32)
+        mhue = np.array([0.4, -1.1, 2.7], np.float32)
     t = np.float32(0.05)
     for m in range(M):
         pos, mat, fib, v, Jp = _particles(sim, m, rng)

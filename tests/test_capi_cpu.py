@@ -62,6 +62,21 @@ def test_null_handle_calls_fail_cleanly(lib):
     assert lib.jf_kernel_launches(None) == -1
 
 
+def test_null_handle_render_calls_fail_cleanly(lib):
+    bad = L.JF_ERR_INVALID
+    assert lib.jf_frame_create(None, 64) == bad
+    assert lib.jf_frame_clear(None, 0.0) == bad
+    assert lib.jf_render_abyss(None, 64, 1, 1.5, None, None, 2) == bad
+    assert lib.jf_render_flat(None, 64, 1, 1.0, 0, 1.0, 1.0, 1.0) == bad
+    assert lib.jf_render_vorticity_overlay(None, 64, 1, 0.001) == bad
+    assert lib.jf_compute_vorticity(None, 0.003) == bad
+    assert lib.jf_render_vorticity(None, 64, 1, 0.6, L.JF_VORT_RDBU) == bad
+    assert lib.jf_tone_map(None) == bad
+    assert lib.jf_read_frame(None, None) == bad
+    assert lib.jf_read_vorticity(None, 0, None) == bad
+    assert lib.jf_write_grid(None, 0, None, None) == bad
+
+
 def test_struct_layout():
     assert ctypes.sizeof(L.JfInstanceDesc) == 16
     assert L.JfConfig.instances.offset == 8 and L.JfConfig.dt.offset == 16

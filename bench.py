@@ -19,7 +19,8 @@ measured HBM copy bandwidth.  ``cpu_baseline`` times the CPU oracle (a
 restatement of the reference's substep) on the host cores.  ``plain`` times
 the plain per-instance launch path on the same inputs.  ``render`` times the
 headless renderer (a 1024^2 viewer frame of every particle) on the final
-state, beside the CPU oracle rendering the same frame.
+state, beside the CPU oracle rendering the same frame.  ``tank`` times one
+generation's tank loading: host-built slot arrays against the GPU water fill.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -324,6 +325,27 @@ def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
             "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast}
 
 
+def tank_leg(engine, M, seed=1000):
+    """One generation's tanks into the engine: host fill_tank + load (slot
+    arrays built on the host and copied) against load_tank (robot on the
+    host, water lattice, exclusion and slot layout on the GPU)."""
+    from jellyfih_b200 import tank
+    genomes = tank.gaussian_genomes(M, seed)
+    t0 = time.perf_counter()
+    for m, g in enumerate(genomes):
+        pos, mat, fib, _ = tank.fill_tank(g, engine.instances[m].n_slots)
+        engine.load(m, pos, mat, fib)
+    engine.sync()
+    host_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for m, g in enumerate(genomes):
+        tank.load_tank(engine, m, g)
+    engine.sync()
+    gpu_s = time.perf_counter() - t0
+    return {"instances": M, "host_fill_and_load_s": host_s, "gpu_fill_s": gpu_s, "speedup": host_s / gpu_s,
+            "note": "per generation; load_tank generates the robot on the host, the water on the GPU"}
+
+
 def render_leg(engine, stream, M, cpu, frames=20, res=1024):
     """One headless frame per step of the reference's viewer pipeline
     (run_population.py:60-65 plus the vorticity views): clear, abyss splats of
@@ -588,6 +610,8 @@ def run_ours(args):
 
         if not args.no_render:
             extras["render"] = render_leg(engine, stream, M, cpu=(rank == 0 and world == 1))
+
+        extras["tank"] = tank_leg(engine, M)
 
         if rank == 0 and world == 1:
             extras["cpu_baseline"] = cpu_baseline(inputs)

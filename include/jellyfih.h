@@ -178,6 +178,19 @@ int jf_write_particles(jf_engine* e, int32_t m, const float* x, const float* v, 
  * grid_v[nx][ny][2], grid_m[nx][ny]; either may be NULL. */
 int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m);
 
+/* Load instance m from its robot alone, with the water filled on the GPU
+ * (make_jelly.py:336-402, fill_tank with no jitter): slots hold the robot
+ * particles (positions rounded to float), then the water lattice of spacing
+ * 1 / (n_grid * spacing_div) between 3/(2 n_grid) of the walls, without every
+ * lattice point within water_margin of a robot particle, in lattice order
+ * (y outer, x inner); water beyond the slots is cut (the robot first, as the
+ * reference truncates), the rest dead.  Then the load reset of
+ * jf_load_instance.  robot_pos [n_robot][2] doubles; robot_fiber may be NULL
+ * (0, 1); out_counts (may be NULL) = {robot particles kept, water particles}. */
+int jf_load_robot(jf_engine* e, int32_t m, const double* robot_pos, const int32_t* robot_mat,
+                  const float* robot_fiber, int32_t n_robot, double water_margin, double spacing_div,
+                  int32_t* out_counts);
+
 /* Overwrite grid_v / grid_m of instance m (grid_v.from_numpy, grid_m.from_numpy;
  * layouts as jf_read_grid).  The next substep recomputes the grid from the
  * particles, so this feeds the renderer and vorticity calls below. */

@@ -68,6 +68,8 @@ EXPORTS = {
     "jf_write_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P]),
     "jf_read_grid": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P]),
     "jf_write_grid": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P]),
+    "jf_load_robot": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, ctypes.c_int32, ctypes.c_double,
+                                     ctypes.c_double, _P]),
     "jf_frame_create": (ctypes.c_int, [_E, ctypes.c_int32]),
     "jf_frame_clear": (ctypes.c_int, [_E, ctypes.c_float]),
     "jf_render_abyss": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _P, _P,

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libjellyfih.so")
-SOURCES = ["jf_capi.cu", "jf_plain.cu", "jf_batched.cu", "jf_noalloc.cu", "jf_grad.cu", "jf_render.cu"]
+SOURCES = ["jf_capi.cu", "jf_plain.cu", "jf_batched.cu", "jf_noalloc.cu", "jf_grad.cu", "jf_render.cu", "jf_tank.cu"]
 HEADERS = ["jf_device.cuh", "jf_engine.h", "jf_dual.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -82,6 +82,20 @@ int upload_params(jf_engine* e) {
   return JF_OK;
 }
 
+// Live count of instance m after a load; the batched path's clusters take
+// instances in descending live count, so that the longest run first when the
+// clusters do not all fit at once.
+int set_live_count(jf_engine* e, int m, int32_t live) {
+  if (!e->d_order) return JF_OK;
+  e->n_live[m] = live;
+  for (int q = 0; q < e->M; ++q) e->h_order[q] = q;
+  std::stable_sort(e->h_order.begin(), e->h_order.end(),
+                   [&](int32_t a, int32_t b) { return e->n_live[a] > e->n_live[b]; });
+  JF_CK(cudaMemcpyAsync(e->d_order, e->h_order.data(), sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream),
+        "cluster order");
+  return JF_OK;
+}
+
 // Instance m's particle arrays in engine order, copied to the host.
 struct HostInstance {
   std::vector<float4> xv, C, F;
@@ -461,20 +475,79 @@ int jf_load_instance(jf_engine* e, int32_t m, const float* pos, const int32_t* m
           "stage material");
   }
   JF_CK(jf_load_launch(e, m, n), "load kernel");
-  if (e->d_order) {
-    // clusters take instances in descending live count, so that the longest
-    // run first when the clusters do not all fit at once
-    int32_t live = 0;
-    for (int k = 0; k < n; ++k) live += material[k] >= 0 ? 1 : 0;
-    e->n_live[m] = live;
-    for (int q = 0; q < e->M; ++q) e->h_order[q] = q;
-    std::stable_sort(e->h_order.begin(), e->h_order.end(),
-                     [&](int32_t a, int32_t b) { return e->n_live[a] > e->n_live[b]; });
-    JF_CK(cudaMemcpyAsync(e->d_order, e->h_order.data(), sizeof(int32_t) * e->M, cudaMemcpyHostToDevice,
-                          e->stream), "cluster order");
-  }
+  int32_t live = 0;
+  for (int k = 0; k < n; ++k) live += material[k] >= 0 ? 1 : 0;
+  if ((rc = set_live_count(e, m, live))) return rc;
   JF_CK(cudaStreamSynchronize(e->stream), "load sync");
   e->sorted = false;
+  return JF_OK;
+}
+
+int jf_load_robot(jf_engine* e, int32_t m, const double* robot_pos, const int32_t* robot_mat,
+                  const float* robot_fiber, int32_t n_robot, double water_margin, double spacing_div,
+                  int32_t* out_counts) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
+  if (n_robot < 0 || (n_robot > 0 && (!robot_pos || !robot_mat)))
+    return fail(e, JF_ERR_INVALID, "robot positions and materials are required");
+  if (!(spacing_div > 0.0) || !(water_margin >= 0.0))
+    return fail(e, JF_ERR_INVALID, "spacing_div must be > 0 and water_margin >= 0");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const JfInst& I = e->inst[m];
+  const size_t S = (size_t)e->max_slots;
+  const int32_t nr = std::min(n_robot, I.n_slots);  // make_jelly.py:371-374: the robot keeps its slots
+  JF_CK(jf_glow_to_slot_order(e, m), "glow reorder");
+  double bbox[4] = {0.0, 0.0, -1.0, -1.0};
+  if (nr > 0) {
+    std::vector<float> pos(2 * (size_t)nr), fib(2 * (size_t)nr);
+    for (int k = 0; k < nr; ++k) {
+      pos[2 * k] = (float)robot_pos[2 * k];
+      pos[2 * k + 1] = (float)robot_pos[2 * k + 1];
+      fib[2 * k] = robot_fiber ? robot_fiber[2 * k] : 0.0f;
+      fib[2 * k + 1] = robot_fiber ? robot_fiber[2 * k + 1] : 1.0f;
+    }
+    JF_CK(cudaMemcpyAsync(e->d_stage, pos.data(), sizeof(float) * pos.size(), cudaMemcpyHostToDevice, e->stream),
+          "stage robot");
+    JF_CK(cudaMemcpyAsync(e->d_stage + 2 * S, fib.data(), sizeof(float) * fib.size(), cudaMemcpyHostToDevice,
+                          e->stream), "stage robot fibre");
+    JF_CK(cudaMemcpyAsync(e->d_stage_i, robot_mat, sizeof(int32_t) * nr, cudaMemcpyHostToDevice, e->stream),
+          "stage robot material");
+  }
+  if (n_robot > 0) {
+    bbox[0] = bbox[2] = robot_pos[0];
+    bbox[1] = bbox[3] = robot_pos[1];
+    for (int k = 1; k < n_robot; ++k) {
+      bbox[0] = std::min(bbox[0], robot_pos[2 * k]);
+      bbox[2] = std::max(bbox[2], robot_pos[2 * k]);
+      bbox[1] = std::min(bbox[1], robot_pos[2 * k + 1]);
+      bbox[3] = std::max(bbox[3], robot_pos[2 * k + 1]);
+    }
+  }
+  // every robot particle excludes water, also those cut from the slots
+  double* d_robot = nullptr;
+  int32_t* d_scratch = nullptr;
+  const int64_t scratch = jf_tank_scratch_ints(e, m, spacing_div);
+  int32_t total = 0;
+  cudaError_t err = alloc(&d_robot, 2 * (size_t)std::max(n_robot, 1));
+  if (err == cudaSuccess) err = alloc(&d_scratch, (size_t)scratch);
+  if (err == cudaSuccess && n_robot > 0)
+    err = cudaMemcpyAsync(d_robot, robot_pos, sizeof(double) * 2 * n_robot, cudaMemcpyHostToDevice, e->stream);
+  if (err == cudaSuccess)
+    err = jf_tank_water_launch(e, m, d_robot, n_robot, bbox, water_margin, spacing_div, d_scratch, scratch, &total);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+  cudaFree(d_robot);
+  cudaFree(d_scratch);
+  if (err != cudaSuccess) return cuda_fail(e, err, "tank water fill");
+  const int32_t n_water = std::max(0, std::min(total, I.n_slots - n_robot));
+  JF_CK(jf_load_launch(e, m, nr + n_water), "load kernel");
+  if ((rc = set_live_count(e, m, nr + n_water))) return rc;
+  JF_CK(cudaStreamSynchronize(e->stream), "load sync");
+  e->sorted = false;
+  if (out_counts) {
+    out_counts[0] = nr;
+    out_counts[1] = n_water;
+  }
   return JF_OK;
 }
 

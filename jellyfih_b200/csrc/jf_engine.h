@@ -165,3 +165,10 @@ cudaError_t jf_render_overlay_launch(jf_engine* e, int res_sub, int grid_side, f
 cudaError_t jf_vorticity_launch(jf_engine* e, float scale);
 cudaError_t jf_render_vort_launch(jf_engine* e, int res_sub, int grid_side, float alpha, int style);
 cudaError_t jf_tone_map_launch(jf_engine* e);
+// Tank fill (jf_tank.cu): water lattice of instance m minus the robot's
+// margin, placed after the robot in the load staging; *h_total = kept
+// candidates (read back on the engine's stream; valid after a sync).
+cudaError_t jf_tank_water_launch(jf_engine* e, int m, const double* d_robot, int n_robot, const double* bbox,
+                                 double water_margin, double spacing_div, int32_t* d_scratch,
+                                 int64_t scratch_ints, int32_t* h_total);
+int64_t jf_tank_scratch_ints(const jf_engine* e, int m, double spacing_div);

@@ -272,6 +272,22 @@ class Engine:
         self._check(self._lib.jf_read_grid(self._h, m, _ptr(gv), _ptr(gm)))
         return gv, gm
 
+    def load_robot(self, m: int, robot_pos, robot_mat, robot_fiber=None, water_margin=0.005,
+                   spacing_div=2.0):
+        """Load instance m from its robot particles with the water filled on
+        the GPU (make_jelly.py:336-402; jf_load_robot): the slot contents of
+        tank.fill_tank without jitter.  Returns (robot particles, water
+        particles) placed."""
+        rp = np.ascontiguousarray(robot_pos, np.float64).reshape(-1, 2)
+        n = len(rp)
+        rm = np.ascontiguousarray(robot_mat, np.int32).reshape(n)
+        rf = None if robot_fiber is None else _f32(robot_fiber, (n, 2))
+        out = np.zeros(2, np.int32)
+        self._check(self._lib.jf_load_robot(self._h, int(m), _ptr(rp) if n else None, _ptr(rm) if n else None,
+                                            _ptr(rf) if n else None, n, float(water_margin), float(spacing_div),
+                                            _ptr(out)))
+        return int(out[0]), int(out[1])
+
     def write_grid(self, m: int, grid_v, grid_m) -> None:
         """grid_v (nx, ny, 2) / grid_m (nx, ny) of instance m (from_numpy)."""
         s = self.instances[m]

@@ -363,6 +363,31 @@ def fill_tank(genome, max_particles, grid_res=128, spawn_offset=None, water_marg
     }
 
 
+def load_tank(engine, m, genome, spawn_offset=None, water_margin=0.005, with_payload=True, spacing_div=2.0,
+              axisym=None):
+    """fill_tank straight into instance m of ``engine``: the robot is generated
+    here (generate_phenotype), the water lattice, its exclusion around the
+    robot and the slot layout run on the GPU (Engine.load_robot).  The slots
+    hold exactly what fill_tank(genome, n_slots, grid_res=n_grid,
+    domain_height=..., jitter=0) returns; the stats dict is fill_tank's."""
+    spec = engine.instances[m]
+    if spawn_offset is None:
+        spawn_offset = DEFAULT_SPAWN
+    robot_pos, robot_mat, robot_fiber, self_intersecting = generate_phenotype(
+        genome, spawn_offset, grid_res=spec.n_grid, with_payload=with_payload, axisym=axisym)
+    n_robot, n_water = engine.load_robot(m, robot_pos, robot_mat, robot_fiber, water_margin, spacing_div)
+    mats = np.asarray(robot_mat[:n_robot])
+    return {
+        'n_robot': n_robot,
+        'n_water': n_water,
+        'n_total': n_robot + n_water,
+        'n_dead': spec.n_slots - n_robot - n_water,
+        'muscle_count': int(np.sum(mats == 3)),
+        'n_jelly': int(np.sum(mats == 1)),
+        'self_intersecting': self_intersecting,
+    }
+
+
 def uniform_genomes(n, seed):
     """n genomes drawn uniformly within the gene bounds (evolve.py:60-61)."""
     rng = np.random.default_rng(seed)

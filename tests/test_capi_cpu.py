@@ -75,6 +75,7 @@ def test_null_handle_render_calls_fail_cleanly(lib):
     assert lib.jf_read_frame(None, None) == bad
     assert lib.jf_read_vorticity(None, 0, None) == bad
     assert lib.jf_write_grid(None, 0, None, None) == bad
+    assert lib.jf_load_robot(None, 0, None, None, None, 0, 0.005, 2.0, None) == bad
 
 
 def test_struct_layout():

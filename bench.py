@@ -240,7 +240,7 @@ def refine_leg(device, stream, M=256, steps=400, iterations=3, checkpoint_every=
     genomes from a seeded Gaussian (CMA-ES style) sample, `iterations` gradient
     steps of 0.05 of the range on the two timing genes (each a checkpointed
     forward + backward of all instances), then the initial and refined genomes
-    re-judged by the plain forward path and the GPU fitness kernel."""
+    re-evaluated by the plain forward path and the GPU fitness kernel."""
     import torch
     from jellyfih_b200 import Engine, InstanceSpec, tank
     from jellyfih_b200.autograd import refine_timing_genes
@@ -262,24 +262,24 @@ def refine_leg(device, stream, M=256, steps=400, iterations=3, checkpoint_every=
     wall = time.perf_counter() - t0
     e.close()
 
-    judge = Engine([spec] * M, path="plain", device=device)
-    judge.set_stream(stream)
+    evaluator = Engine([spec] * M, path="plain", device=device)
+    evaluator.set_stream(stream)
     fits = {}
     for name, g in (("initial", genomes), ("refined", refined)):
         for m in range(M):
-            judge.load(m, pos[m], mats[m], fibs[m])
+            evaluator.load(m, pos[m], mats[m], fibs[m])
         c = np.clip(g[:, 9], 0.05, 0.60)
-        judge.set_params(contraction=c, freq=np.clip(g[:, 10], 0.5, 2.0))
-        rows = judge.run_headless(steps)
+        evaluator.set_params(contraction=c, freq=np.clip(g[:, 10], 0.5, 2.0))
+        rows = evaluator.run_headless(steps)
         fits[name] = {"mean_displacement": float(np.mean(rows[:, 2] - rows[:, 0])),
-                      "fitness": judge.fitness(rows, muscle, c, mode="displacement")}
-    judge.close()
+                      "fitness": evaluator.fitness(rows, muscle, c, mode="displacement")}
+    evaluator.close()
     better = float(np.mean(fits["refined"]["fitness"] < fits["initial"]["fitness"]))
     return {"instances": M, "grid": "64x64", "slots": 20000, "live_per_instance": float(np.mean([(m >= 0).sum() for m in mats])),
             "substeps": steps, "checkpoint_every": checkpoint_every, "gradient_steps": iterations,
             "s_per_gradient_step": wall / iterations,
             "mean_displacement_per_step": [float(np.mean(h)) for h in hist],
-            "plain_judge": {"initial_mean_displacement": fits["initial"]["mean_displacement"],
+            "plain_evaluation": {"initial_mean_displacement": fits["initial"]["mean_displacement"],
                             "refined_mean_displacement": fits["refined"]["mean_displacement"],
                             "fraction_with_better_fitness": better}}
 
@@ -581,7 +581,7 @@ def run_ours(args):
             from jellyfih_b200.shard import gather_rows
             extras["e2e"]["gathered_results"] = int(gather_rows(res).shape[0])
 
-        # plain per-instance launch path on the same inputs (BASELINE: batched vs plain)
+        # plain per-instance launch path on the same inputs (the batched / plain ratio)
         plain = Engine([spec] * M, path="plain", device=local)
         plain.set_stream(stream)
         load_all(plain, inputs)

@@ -342,8 +342,19 @@ def tank_leg(engine, M, seed=1000):
         tank.load_tank(engine, m, g)
     engine.sync()
     gpu_s = time.perf_counter() - t0
-    return {"instances": M, "host_fill_and_load_s": host_s, "gpu_fill_s": gpu_s, "speedup": host_s / gpu_s,
-            "note": "per generation; load_tank generates the robot on the host, the water on the GPU"}
+    pool = tank.make_pool()
+    try:
+        tank.load_tanks(engine, genomes, executor=pool)  # starts the workers
+        t0 = time.perf_counter()
+        tank.load_tanks(engine, genomes, executor=pool)
+        engine.sync()
+        pool_s = time.perf_counter() - t0
+    finally:
+        pool.shutdown()
+    return {"instances": M, "host_fill_and_load_s": host_s, "gpu_fill_s": gpu_s,
+            "gpu_fill_pooled_robots_s": pool_s, "workers": os.cpu_count(), "speedup": host_s / pool_s,
+            "note": "per generation; load_tank generates the robot on the host, the water on the GPU; "
+                    "the pooled run spreads the robots over spawned worker processes"}
 
 
 def render_leg(engine, stream, M, cpu, frames=20, res=1024):

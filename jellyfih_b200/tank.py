@@ -363,6 +363,64 @@ def fill_tank(genome, max_particles, grid_res=128, spawn_offset=None, water_marg
     }
 
 
+def _phenotype_job(args):
+    genome, spawn_offset, grid_res, with_payload, axisym = args
+    return generate_phenotype(genome, spawn_offset, grid_res=grid_res, with_payload=with_payload, axisym=axisym)
+
+
+def make_pool(workers=None):
+    """A process pool for phenotypes(): spawned workers (they inherit no CUDA
+    state and import only numpy and scipy).  Reuse it across generations;
+    close it with .shutdown().  Spawned workers import the caller's main
+    module, so a script that uses the pool keeps its top-level work under
+    ``if __name__ == "__main__":``."""
+    import concurrent.futures
+    import multiprocessing
+    return concurrent.futures.ProcessPoolExecutor(max_workers=workers or os.cpu_count(),
+                                                  mp_context=multiprocessing.get_context("spawn"))
+
+
+def phenotypes(genomes, spawn_offset=None, grid_res=128, with_payload=True, axisym=None, executor=None):
+    """generate_phenotype of every genome, in order; with an ``executor``
+    (make_pool()) the genomes are spread over its worker processes.  The
+    results are those of the serial calls (same float64 operations)."""
+    if spawn_offset is None:
+        spawn_offset = DEFAULT_SPAWN
+    axisym = _axisym_default(axisym)  # resolved here, not from the workers' environment
+    res = grid_res if np.ndim(grid_res) else [grid_res] * len(genomes)
+    jobs = [(g, spawn_offset, int(r), with_payload, axisym) for g, r in zip(genomes, res)]
+    if executor is None:
+        return [_phenotype_job(j) for j in jobs]
+    workers = getattr(executor, "_max_workers", None) or os.cpu_count() or 1
+    return list(executor.map(_phenotype_job, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
+
+
+def _tank_stats(engine, m, robot_mat, n_robot, n_water, self_intersecting):
+    mats = np.asarray(robot_mat[:n_robot])
+    return {
+        'n_robot': n_robot,
+        'n_water': n_water,
+        'n_total': n_robot + n_water,
+        'n_dead': engine.instances[m].n_slots - n_robot - n_water,
+        'muscle_count': int(np.sum(mats == 3)),
+        'n_jelly': int(np.sum(mats == 1)),
+        'self_intersecting': self_intersecting,
+    }
+
+
+def load_tanks(engine, genomes, spawn_offset=None, water_margin=0.005, with_payload=True, spacing_div=2.0,
+               axisym=None, executor=None):
+    """load_tank for instances 0 .. len(genomes) - 1, the robots generated
+    first (over ``executor``'s workers when given); returns the stats dicts."""
+    robots = phenotypes(genomes, spawn_offset, [engine.instances[m].n_grid for m in range(len(genomes))],
+                        with_payload, axisym, executor)
+    out = []
+    for m, (rp, rm, rf, si) in enumerate(robots):
+        n_robot, n_water = engine.load_robot(m, rp, rm, rf, water_margin, spacing_div)
+        out.append(_tank_stats(engine, m, rm, n_robot, n_water, si))
+    return out
+
+
 def load_tank(engine, m, genome, spawn_offset=None, water_margin=0.005, with_payload=True, spacing_div=2.0,
               axisym=None):
     """fill_tank straight into instance m of ``engine``: the robot is generated
@@ -376,16 +434,7 @@ def load_tank(engine, m, genome, spawn_offset=None, water_margin=0.005, with_pay
     robot_pos, robot_mat, robot_fiber, self_intersecting = generate_phenotype(
         genome, spawn_offset, grid_res=spec.n_grid, with_payload=with_payload, axisym=axisym)
     n_robot, n_water = engine.load_robot(m, robot_pos, robot_mat, robot_fiber, water_margin, spacing_div)
-    mats = np.asarray(robot_mat[:n_robot])
-    return {
-        'n_robot': n_robot,
-        'n_water': n_water,
-        'n_total': n_robot + n_water,
-        'n_dead': spec.n_slots - n_robot - n_water,
-        'muscle_count': int(np.sum(mats == 3)),
-        'n_jelly': int(np.sum(mats == 1)),
-        'self_intersecting': self_intersecting,
-    }
+    return _tank_stats(engine, m, robot_mat, n_robot, n_water, self_intersecting)
 
 
 def uniform_genomes(n, seed):

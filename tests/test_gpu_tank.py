@@ -105,3 +105,20 @@ def test_gpu_tank_then_step_runs():
     finally:
         a.close()
         b.close()
+
+
+def test_gpu_tanks_over_a_pool_match_host_fill():
+    """load_tanks with the robots generated over spawned workers: every
+    instance's slots equal fill_tank's."""
+    from jellyfih_b200 import Engine, InstanceSpec, tank
+    genomes = tank.gaussian_genomes(4, 55)
+    e = Engine([InstanceSpec(80000)] * 4, path="batched")
+    pool = tank.make_pool(2)
+    try:
+        stats = tank.load_tanks(e, genomes, executor=pool)
+        for m, g in enumerate(genomes):
+            fx = tank.fill_tank(g, 80000)
+            _compare(e, m, fx, fx[3], stats[m])
+    finally:
+        pool.shutdown()
+        e.close()

@@ -105,3 +105,21 @@ def test_vectorised_self_intersection_matches_the_pair_loop():
     for g in tank.uniform_genomes(8, 5):
         pos, mat, fib, st = tank.fill_tank(g, 80000)
         assert isinstance(st["self_intersecting"], bool)
+
+
+def test_phenotypes_over_a_process_pool_match_serial():
+    """generate_phenotype spread over spawned workers returns the serial
+    results bit for bit, in genome order."""
+    from jellyfih_b200 import tank
+    genomes = tank.gaussian_genomes(6, 21)
+    serial = tank.phenotypes(genomes, grid_res=[128, 64, 128, 64, 128, 128])
+    pool = tank.make_pool(2)
+    try:
+        pooled = tank.phenotypes(genomes, grid_res=[128, 64, 128, 64, 128, 128], executor=pool)
+    finally:
+        pool.shutdown()
+    assert len(pooled) == len(serial)
+    for a, b in zip(serial, pooled):
+        for x, y in zip(a[:3], b[:3]):
+            np.testing.assert_array_equal(x, y)
+        assert a[3] == b[3]

@@ -325,7 +325,7 @@ def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
             "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast}
 
 
-def tank_leg(engine, M, seed=1000):
+def tank_leg(engine, M, seed=1000, workers=None):
     """One generation's tanks into the engine: host fill_tank + load (slot
     arrays built on the host and copied) against load_tank (robot on the
     host, water lattice, exclusion and slot layout on the GPU)."""
@@ -342,7 +342,8 @@ def tank_leg(engine, M, seed=1000):
         tank.load_tank(engine, m, g)
     engine.sync()
     gpu_s = time.perf_counter() - t0
-    pool = tank.make_pool()
+    workers = workers or os.cpu_count() or 1
+    pool = tank.make_pool(workers)
     try:
         tank.load_tanks(engine, genomes, executor=pool)  # starts the workers
         t0 = time.perf_counter()
@@ -352,7 +353,7 @@ def tank_leg(engine, M, seed=1000):
     finally:
         pool.shutdown()
     return {"instances": M, "host_fill_and_load_s": host_s, "gpu_fill_s": gpu_s,
-            "gpu_fill_pooled_robots_s": pool_s, "workers": os.cpu_count(), "speedup": host_s / pool_s,
+            "gpu_fill_pooled_robots_s": pool_s, "workers": workers, "speedup": host_s / pool_s,
             "note": "per generation; load_tank generates the robot on the host, the water on the GPU; "
                     "the pooled run spreads the robots over spawned worker processes"}
 
@@ -622,7 +623,8 @@ def run_ours(args):
         if not args.no_render:
             extras["render"] = render_leg(engine, stream, M, cpu=(rank == 0 and world == 1))
 
-        extras["tank"] = tank_leg(engine, M)
+        # the host's cores are shared by the ranks of this node
+        extras["tank"] = tank_leg(engine, M, workers=max(1, (os.cpu_count() or 1) // world))
 
         if rank == 0 and world == 1:
             extras["cpu_baseline"] = cpu_baseline(inputs)

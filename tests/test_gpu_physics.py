@@ -1,0 +1,97 @@
+"""The reference's physical sanity runs (evolve.py:158-245), the only
+known-answer checks it has, on the GPU:
+
+* payload-sink baseline (evolve.py:189-245): a payload rectangle without a
+  jellyfish, centred at (0.5, 0.5) in the water lattice, must sink more than
+  0.005 over 20,000 substeps;
+* zero-actuation baseline (evolve.py:158-186): the centre genome with
+  actuation 0 must drift by at most 0.05 over 20,000 substeps.
+
+The payload tank is built here as evolve.py builds it (payload raster at
+2 points per cell, water lattice of spacing 1/256 minus a 0.005 margin around
+the payload) and, in a second engine, by the GPU tank fill from the payload
+alone: both give the same slots.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+STEPS = 20000
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import build
+    build.build()
+
+
+def _payload_tank(n_slots, n_grid=128):
+    """evolve.py:197-232 restated: payload raster, water lattice, slots."""
+    from scipy.spatial import cKDTree
+    from jellyfih_b200 import tank
+    spacing = 1.0 / (n_grid * 2.0)
+    margin = spacing * 3
+    raster_res = n_grid * 2
+    px = np.linspace(-tank.PAYLOAD_WIDTH / 2, tank.PAYLOAD_WIDTH / 2, int(tank.PAYLOAD_WIDTH * raster_res))
+    py = np.linspace(0, tank.PAYLOAD_HEIGHT, int(tank.PAYLOAD_HEIGHT * raster_res))
+    pgx, pgy = np.meshgrid(px, py)
+    payload = np.vstack([pgx.ravel(), pgy.ravel()]).T + np.array([0.5, 0.5])
+    wx = np.arange(margin, 1.0 - margin, spacing)
+    wy = np.arange(margin, 1.0 - margin, spacing)
+    wgx, wgy = np.meshgrid(wx, wy)
+    cand = np.vstack([wgx.ravel(), wgy.ravel()]).T
+    d, _ = cKDTree(payload).query(cand, k=1)
+    water = cand[d > 0.005]
+    n_p = len(payload)
+    n_w = min(len(water), n_slots - n_p)
+    pos = np.full((n_slots, 2), -1.0, np.float32)
+    mat = np.full(n_slots, -1, np.int32)
+    fib = np.zeros((n_slots, 2), np.float32)
+    fib[:, 1] = 1.0
+    pos[:n_p] = payload
+    mat[:n_p] = 2
+    pos[n_p:n_p + n_w] = water[:n_w]
+    mat[n_p:n_p + n_w] = 0
+    return payload, pos, mat, fib
+
+
+@pytest.mark.parametrize("path", ("plain", "batched"))
+def test_payload_sinks_without_jellyfish(path):
+    from jellyfih_b200 import Engine, InstanceSpec
+    payload, pos, mat, fib = _payload_tank(80000)
+    host = Engine([InstanceSpec(80000)], path=path)
+    gpu = Engine([InstanceSpec(80000)], path=path)
+    try:
+        host.load(0, pos, mat, fib)
+        gpu.load_robot(0, payload, np.full(len(payload), 2, np.int32))
+        for k in ("x", "material", "fiber"):
+            np.testing.assert_array_equal(gpu.read(0)[k], host.read(0)[k])
+        rows = host.run_headless(STEPS)
+        disp = rows[0, 2] - rows[0, 0]
+        assert disp < -0.005, f"payload moved {disp:+.4f} (the reference expects it to sink)"
+        assert rows[0, 4] == 1.0
+    finally:
+        host.close()
+        gpu.close()
+
+
+def test_passive_centre_genome_barely_drifts():
+    from jellyfih_b200 import Engine, InstanceSpec, tank
+    g = (tank.GENOME_LOWER + tank.GENOME_UPPER) / 2  # evolve.py:60-63
+    g[9], g[10] = 0.20, 1.0
+    e = Engine([InstanceSpec(80000)], path="batched")
+    try:
+        tank.load_tank(e, 0, g)
+        c, f = tank.timing_params(g)
+        e.set_params(actuation=0.0, contraction=c, freq=f)
+        e.time = 0.0
+        rows = e.run_headless(STEPS)
+        disp = rows[0, 2] - rows[0, 0]
+        assert abs(disp) <= 0.05, f"passive body drifted {disp:+.4f} with zero actuation"
+        assert np.isfinite(rows).all()
+    finally:
+        e.close()

@@ -82,18 +82,24 @@ int upload_params(jf_engine* e) {
   return JF_OK;
 }
 
-// Live count of instance m after a load; the batched path's clusters take
-// instances in descending live count, so that the longest run first when the
-// clusters do not all fit at once.
-int set_live_count(jf_engine* e, int m, int32_t live) {
+// The batched path's clusters take instances in descending live count
+// (e->n_live), so that the longest run first when the clusters do not all
+// fit at once: re-sorts the order and queues its upload.
+int upload_order(jf_engine* e) {
   if (!e->d_order) return JF_OK;
-  e->n_live[m] = live;
   for (int q = 0; q < e->M; ++q) e->h_order[q] = q;
   std::stable_sort(e->h_order.begin(), e->h_order.end(),
                    [&](int32_t a, int32_t b) { return e->n_live[a] > e->n_live[b]; });
   JF_CK(cudaMemcpyAsync(e->d_order, e->h_order.data(), sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream),
         "cluster order");
   return JF_OK;
+}
+
+// Live count of instance m after a load, and the cluster order with it.
+int set_live_count(jf_engine* e, int m, int32_t live) {
+  if (!e->d_order) return JF_OK;
+  e->n_live[m] = live;
+  return upload_order(e);
 }
 
 // Instance m's particle arrays in engine order, copied to the host.
@@ -732,11 +738,8 @@ int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, cons
       for (int32_t k = 0; k < I.n_slots; ++k) live += material[I.p_off + k] >= 0 ? 1 : 0;
       e->n_live[m] = live;
     }
-    for (size_t q = 0; q < M; ++q) e->h_order[q] = (int32_t)q;
-    std::stable_sort(e->h_order.begin(), e->h_order.end(),
-                     [&](int32_t a, int32_t b) { return e->n_live[a] > e->n_live[b]; });
-    JF_CK(cudaMemcpyAsync(e->d_order, e->h_order.data(), sizeof(int32_t) * M, cudaMemcpyHostToDevice, e->stream),
-          "cluster order");
+    int rc = upload_order(e);
+    if (rc) return rc;
   }
   // timing genes (evolve.py:150-152)
   for (size_t m = 0; m < M; ++m) {

@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-render", action="store_true", help="skip the headless-renderer leg")
     ap.add_argument("--render-only", action="store_true",
                     help="run only the renderer leg on the workload after --substeps substeps and print it")
+    ap.add_argument("--grad-substeps", type=int, default=2000,
+                    help="substeps of the differentiable rollout leg (checkpoint every 100)")
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiable leg (8 of the workload's instances) and print it")
     return ap.parse_args()
@@ -284,9 +286,9 @@ def refine_leg(device, stream, M=256, steps=400, iterations=3, checkpoint_every=
                             "fraction_with_better_fitness": better}}
 
 
-def grad_leg(inputs, device, stream, steps=200, checkpoint_every=100):
+def grad_leg(inputs, device, stream, steps=2000, checkpoint_every=100):
     """fwd+bwd / fwd of the differentiable rollout: 8 instances x 80,000 slots,
-    `steps` substeps (a bounded sample of the 2,000-substep rollout), device
+    2,000 substeps with a checkpoint every 100 (the gradient workload), device
     time of the checkpointed forward and of the backward (recompute + adjoint)."""
     import torch
     from jellyfih_b200 import Engine, InstanceSpec
@@ -613,7 +615,7 @@ def run_ours(args):
                            "ms_per_substep": pms / P,
                            "batched_over_plain": value / plain_value}
 
-        extras["differentiable"] = grad_leg(inputs[:8], local, stream)
+        extras["differentiable"] = grad_leg(inputs[:8], local, stream, steps=args.grad_substeps)
         if not args.no_refine:
             extras["refine"] = refine_leg(local, stream)
 
@@ -657,7 +659,7 @@ def run_grad_only(args):
     torch.cuda.set_device(0)
     inputs = make_inputs(args.instances, args.slots, 1000)
     stream = torch.cuda.Stream()
-    out = {"differentiable": grad_leg(inputs[:8], 0, stream)}
+    out = {"differentiable": grad_leg(inputs[:8], 0, stream, steps=args.grad_substeps)}
     if not args.no_refine:
         out["refine"] = refine_leg(0, stream)
     print(json.dumps(out), flush=True)

@@ -578,6 +578,8 @@ def run_ours(args):
         mus = np.array([i[5]["muscle_count"] for i in inputs], np.int32)
         h2d = pos_all.nbytes + mat_all.nbytes + fib_all.nbytes + con.nbytes + frq.nbytes + mus.nbytes
         e2e_steps = max(2, K // 4)
+        # one untimed episode first: the call allocates its staging buffers once
+        engine.run_episode(pos_all, mat_all, con, S, fibers=fib_all, freq=frq, muscle_counts=mus)
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()

@@ -44,8 +44,14 @@ constexpr int kMaxCluster = 16;
 // into CS bands of about equal cost (cell-loop iterations at the chosen cap,
 // overflow, grid update), each at most band_cap rows (the shared-memory
 // window's capacity).  Grids taller than kMaxBandRows keep equal-height bands.
-constexpr int kMaxBandRows = 1024;
+constexpr int kMaxBandRows = kJfMaxBandRows;
 constexpr int kRowCost = 40;  // grid update of one row, in the cost model's units
+// A non-water particle takes the full SVD and stress path, which the whole
+// warp of its cell segment then executes; robot cells are mostly full of
+// such particles, so the extra cost spread over them is small: 1.5 units per
+// particle (in half units here; measured best among 1 / 1.5 / 2 / 3 / 4 / 8,
+// 2.3 % on the 32-instance batch against no weight).
+constexpr int kSolidCostHalves = 3;
 constexpr int kNoCap = 1 << 30;
 
 // Sort cell of a particle: (floor(X - 1/4), floor(Y - 1/4)) in grid units,
@@ -563,7 +569,8 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
 // particles outside the stencil range and one for dead slots.
 __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* __restrict__ xv,
                                  const int32_t* __restrict__ mat, int32_t* __restrict__ keys,
-                                 int32_t* __restrict__ rank, int32_t* __restrict__ counts, int stride) {
+                                 int32_t* __restrict__ rank, int32_t* __restrict__ counts, int stride,
+                                 int32_t* __restrict__ solid) {
   const int m = blockIdx.y;
   const JfInst I = inst[m];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -571,7 +578,8 @@ __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* 
   const int64_t g = I.p_off + k;
   const int cells = I.nx * I.ny;
   int key;
-  if (mat[g] < 0) {
+  const int mt = mat[g];
+  if (mt < 0) {
     key = cells + 1;
   } else {
     const float4 a = xv[g];
@@ -585,6 +593,7 @@ __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* 
   }
   keys[g] = key;
   rank[g] = atomicAdd(counts + (int64_t)m * stride + key, 1);
+  if (mt > 0 && key < cells && I.ny <= kMaxBandRows) atomicAdd(solid + m * kMaxBandRows + key / I.nx, 1);
 }
 
 // Per instance: the cell cap, the exclusive scan of the bins (counts become
@@ -598,7 +607,7 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
                                                                 int32_t* __restrict__ cap_out,
                                                                 int32_t* __restrict__ ovband,
                                                                 int32_t* __restrict__ ovcur, int CS,
-                                                                int fixed_cap) {
+                                                                int fixed_cap, const int32_t* __restrict__ solid) {
   __shared__ int warp_sums[kScanThreads / 32];
   __shared__ int s_cost[kCapCandidates];
   __shared__ int s_row_cost[kMaxBandRows];
@@ -617,7 +626,7 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
   // quarter lane-iterations: 128 per warp iteration, 6 per overflow particle
   if (threadIdx.x < kCapCandidates) s_cost[threadIdx.x] = 0;
   for (int y = threadIdx.x; y < min(I.ny, kMaxBandRows); y += kScanThreads) {
-    s_row_cost[y] = kRowCost;
+    s_row_cost[y] = kRowCost + (kSolidCostHalves * solid[m * kMaxBandRows + y]) / 2;
     s_row_over[y] = 0;
   }
   __syncthreads();
@@ -817,14 +826,16 @@ cudaError_t jf_batched_sort(jf_engine* e) {
   const int stride = e->max_cells + 2;
   cudaError_t err = cudaMemsetAsync(e->d_counts, 0, sizeof(int32_t) * (size_t)stride * e->M, e->stream);
   if (err != cudaSuccess) return err;
+  err = cudaMemsetAsync(e->d_solid, 0, sizeof(int32_t) * (size_t)kMaxBandRows * e->M, e->stream);
+  if (err != cudaSuccess) return err;
   const dim3 grid((e->max_slots + kSortThreads - 1) / kSortThreads, e->M);
   if (e->max_slots > 0) {
     sort_keys_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->p.xv, e->p.mat, e->d_keys,
-                                                          e->d_rank, e->d_counts, stride);
+                                                          e->d_rank, e->d_counts, stride, e->d_solid);
   }
   sort_scan_kernel<<<e->M, kScanThreads, 0, e->stream>>>(e->d_inst, e->d_counts, stride, e->d_band,
                                                          e->d_brow, e->d_cap, e->d_ovband, e->d_ovcur,
-                                                         e->cluster, e->cell_cap);
+                                                         e->cluster, e->cell_cap, e->d_solid);
   if (e->max_slots > 0) {
     sort_scatter_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->d_keys, e->d_rank, e->d_counts,
                                                              stride, e->d_cap, e->cluster, e->d_brow,

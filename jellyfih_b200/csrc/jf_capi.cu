@@ -379,6 +379,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
         (err = alloc(&e->d_cap, e->M)) != cudaSuccess ||
         (err = alloc(&e->d_order, e->M)) != cudaSuccess ||
         (err = alloc(&e->d_brow, (size_t)(e->cluster + 1) * e->M)) != cudaSuccess ||
+        (err = alloc(&e->d_solid, (size_t)kJfMaxBandRows * e->M)) != cudaSuccess ||
         (err = alloc(&e->d_path, 4)) != cudaSuccess ||
         (err = alloc(&e->d_time, 1)) != cudaSuccess ||
         (err = cudaMemset(e->d_path, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
@@ -425,7 +426,7 @@ int jf_destroy(jf_engine* e) {
   free_particles(e->q);
   cudaFree(e->d_inst); cudaFree(e->d_params); cudaFree(e->d_keys); cudaFree(e->d_counts);
   cudaFree(e->d_rank); cudaFree(e->d_ovlist); cudaFree(e->d_ovband); cudaFree(e->d_ovcur);
-  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_brow); cudaFree(e->d_ep); cudaFree(e->d_ep_mat);
+  cudaFree(e->d_band); cudaFree(e->d_cap); cudaFree(e->d_order); cudaFree(e->d_brow); cudaFree(e->d_solid); cudaFree(e->d_ep); cudaFree(e->d_ep_mat);
   cudaFree(e->d_ep_stats); cudaFree(e->d_grid); cudaFree(e->d_stats); cudaFree(e->d_err);
   cudaFree(e->d_stage); cudaFree(e->d_stage_i); cudaFree(e->d_path);
   cudaFree(e->d_fit); cudaFree(e->d_fit_f); cudaFree(e->d_fit_i); cudaFree(e->d_time);

@@ -27,6 +27,9 @@ struct JfParticles {
 };
 
 struct JfGrad;
+// Grids up to this many rows get bands balanced by per-row cost at each
+// re-sort (taller grids keep equal bands).
+constexpr int kJfMaxBandRows = 1024;
 
 struct jf_engine {
   int device = 0;
@@ -69,6 +72,7 @@ struct jf_engine {
   std::vector<int32_t> n_live;     // live particles per instance at its last load
   std::vector<int32_t> h_order;    // host copy of d_order
   int32_t cell_cap = 0;            // batched path: fixed cell cap, 0 = cost model per re-sort
+  int32_t* d_solid = nullptr;      // batched path: M x kJfMaxBandRows non-water particles per grid row
   float4* d_grid = nullptr;        // grid nodes (node = g_off + j * nx + i): (v0, v1, m, 0)
   double* d_stats = nullptr;       // M x 6 CoM sums (payload y, count, x; body y, count, x)
   int32_t* d_err = nullptr;        // per-instance non-finite flags

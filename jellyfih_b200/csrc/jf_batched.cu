@@ -111,6 +111,25 @@ struct Window {
   const int* brow;  // shared copy of the instance's band row starts (CS + 1)
 };
 
+// Distributed shared memory in explicit shared::cluster form: the address of
+// a local shared location in CTA `rank` of the cluster (mapa), and 32-bit
+// loads / reductions there, so that no generic pointer into another CTA's
+// window reaches the code that works on this CTA's window.
+__device__ __forceinline__ uint32_t dsmem_addr(const void* local, int rank) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(local);
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void dsmem_add(uint32_t a, float v) {
+  asm volatile("red.shared::cluster.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ float2 dsmem_ld2(uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
+  return v;
+}
+
 // the band (CTA of the cluster) that owns grid row j, and j's row in its window
 __device__ __forceinline__ int owner_of(const Window& w, int j) {
   int o = 0;
@@ -127,7 +146,7 @@ __device__ __forceinline__ float2 gather_node(const Window& w, cg::cluster_group
   }
   const int o = owner_of(w, j);
   const int n = owner_row(w, j, o) * w.nx + i;
-  return cl.map_shared_rank(w.G, o)[n];
+  return dsmem_ld2(dsmem_addr(w.G + n, o));
 }
 
 // Scatter of one particle's 9 stencil contributions with atomics, local when
@@ -138,23 +157,27 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
   for (int j = 0; j < 3; ++j) {
     const int row = st.by + j;
     const int wr = row - w.win0;
-    float *px = w.Ax, *py = w.Ay, *pm = w.Am, *ph = w.Ah;
-    int rn = wr * w.nx;
-    if (!(wr >= 0 && wr < w.VR)) {
-      const int o = owner_of(w, row);
-      px = cl.map_shared_rank(w.Ax, o);
-      py = cl.map_shared_rank(w.Ay, o);
-      pm = cl.map_shared_rank(w.Am, o);
-      if (I.axisym) ph = cl.map_shared_rank(w.Ah, o);
-      rn = owner_row(w, row, o) * w.nx;
-    }
+    if (wr >= 0 && wr < w.VR) {
+      const int rn = wr * w.nx + st.bx;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const float3 c = jf_node_contrib(I, st, sc, i, j);
-      atomicAdd(px + rn + st.bx + i, c.x);
-      atomicAdd(py + rn + st.bx + i, c.y);
-      atomicAdd(pm + rn + st.bx + i, c.z);
-      if (I.axisym) atomicAdd(ph + rn + st.bx + i, jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
+      for (int i = 0; i < 3; ++i) {
+        const float3 c = jf_node_contrib(I, st, sc, i, j);
+        atomicAdd(w.Ax + rn + i, c.x);
+        atomicAdd(w.Ay + rn + i, c.y);
+        atomicAdd(w.Am + rn + i, c.z);
+        if (I.axisym) atomicAdd(w.Ah + rn + i, jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
+      }
+    } else {
+      const int o = owner_of(w, row);
+      const int rn = owner_row(w, row, o) * w.nx + st.bx;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const float3 c = jf_node_contrib(I, st, sc, i, j);
+        dsmem_add(dsmem_addr(w.Ax + rn + i, o), c.x);
+        dsmem_add(dsmem_addr(w.Ay + rn + i, o), c.y);
+        dsmem_add(dsmem_addr(w.Am + rn + i, o), c.z);
+        if (I.axisym) dsmem_add(dsmem_addr(w.Ah + rn + i, o), jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
+      }
     }
   }
 }
@@ -489,14 +512,14 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         if (vx != 0.0f || vy != 0.0f || vm != 0.0f || vh != 0.0f) {
           const int o = owner_of(w, j);
           const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
-          atomicAdd(cluster.map_shared_rank(w.Ax, o) + rn, vx);
-          atomicAdd(cluster.map_shared_rank(w.Ay, o) + rn, vy);
-          atomicAdd(cluster.map_shared_rank(w.Am, o) + rn, vm);
+          dsmem_add(dsmem_addr(w.Ax + rn, o), vx);
+          dsmem_add(dsmem_addr(w.Ay + rn, o), vy);
+          dsmem_add(dsmem_addr(w.Am + rn, o), vm);
           w.Ax[n] = 0.0f;
           w.Ay[n] = 0.0f;
           w.Am[n] = 0.0f;
           if (I.axisym) {
-            atomicAdd(cluster.map_shared_rank(w.Ah, o) + rn, vh);
+            dsmem_add(dsmem_addr(w.Ah + rn, o), vh);
             w.Ah[n] = 0.0f;
           }
         }
@@ -538,7 +561,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         const int n = wr * nx + (q - h * nx);
         const int o = owner_of(w, j);
         const int rn = owner_row(w, j, o) * nx + (n - wr * nx);
-        w.G[n] = cluster.map_shared_rank(w.G, o)[rn];
+        w.G[n] = dsmem_ld2(dsmem_addr(w.G + rn, o));
       }
       t = t + a.dt;
       if (tid == 0) {

@@ -68,44 +68,97 @@ __device__ __forceinline__ float block_pressure(const GradArgs& a, int m) {
   return s_p;
 }
 
-__global__ void gf_p2g(GradArgs a) {
+// Deterministic P2G.  A block's particles (consecutive slots of one
+// instance) first add their fixed-point contributions into a shared-memory
+// tile covering the block's stencil bounding box, when that box has at most
+// kTileNodes nodes, and the tile then goes to the grid with one atomic per
+// touched node and component; otherwise each contribution goes to the grid
+// directly.  The contributions are integers, so every grouping gives the same
+// sums bit for bit.
+constexpr int kTileNodes = 1024;
+
+__global__ void __launch_bounds__(kT) gf_p2g(GradArgs a) {
+  __shared__ unsigned long long s_acc[3 * kTileNodes];
+  __shared__ int s_box[4];  // stencil bases: min x, min y, max x, max y
   const int m = blockIdx.y;
   const float pressure = block_pressure(a, m);
   const JfInst I = a.inst[m];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= I.n_slots) return;
   const int64_t g = I.p_off + k;
-  const int mt = a.mat[g];
   const bool copy = a.o.F != a.s.F;
-  if (mt < 0) {
-    if (copy) a.o.F[g] = a.s.F[g];
-    return;
-  }
-  const float4 xv = a.s.xv[g];
+  bool valid = false;
   JfStencil st;
-  if (!jf_stencil(I, make_float2(xv.x, xv.y), st)) {
-    if (copy) a.o.F[g] = a.s.F[g];
+  JfScatter sc;
+  if (k < I.n_slots) {
+    const int mt = a.mat[g];
+    const float4 xv = mt >= 0 ? a.s.xv[g] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (mt >= 0 && jf_stencil(I, make_float2(xv.x, xv.y), st)) {
+      float4 F = a.s.F[g];
+      float jp = (mt == 2) ? a.Jp[g] : 1.0f;
+      const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+      jf_p2g_particle(I, a.mats, mt, make_float2(xv.z, xv.w), a.s.C[g], F, jp, fb, pressure,
+                      a.params[m].payload_density, sc);
+      a.o.F[g] = F;
+      if (mt == 2) a.Jp[g] = jp;
+      valid = true;
+    } else if (copy) {
+      a.o.F[g] = a.s.F[g];
+    }
+  }
+  if (threadIdx.x == 0) {
+    s_box[0] = s_box[1] = 0x7fffffff;
+    s_box[2] = s_box[3] = -1;
+  }
+  __syncthreads();
+  if (valid) {
+    atomicMin(&s_box[0], st.bx);
+    atomicMin(&s_box[1], st.by);
+    atomicMax(&s_box[2], st.bx);
+    atomicMax(&s_box[3], st.by);
+  }
+  __syncthreads();
+  const int x0 = s_box[0], y0 = s_box[1];
+  const int W = s_box[2] - x0 + 3, H = s_box[3] - y0 + 3;
+  if (s_box[2] < 0) return;  // no particle of the block scatters (uniform)
+  unsigned long long* fix = a.fix + 3 * I.g_off;
+  if (W * H > kTileNodes) {  // uniform: the direct path
+    if (!valid) return;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float3 c = jf_node_contrib(I, st, sc, i, j);
+        const int64_t n = 3 * ((int64_t)(st.by + j) * I.nx + st.bx + i);
+        add_fixed(fix + n + 0, c.x);
+        add_fixed(fix + n + 1, c.y);
+        add_fixed(fix + n + 2, c.z);
+      }
+    }
     return;
   }
-  float4 F = a.s.F[g];
-  float jp = (mt == 2) ? a.Jp[g] : 1.0f;
-  const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
-  JfScatter sc;
-  jf_p2g_particle(I, a.mats, mt, make_float2(xv.z, xv.w), a.s.C[g], F, jp, fb, pressure,
-                  a.params[m].payload_density, sc);
-  a.o.F[g] = F;
-  if (mt == 2) a.Jp[g] = jp;
-  unsigned long long* fix = a.fix + 3 * I.g_off;
+  const int entries = 3 * W * H;
+  for (int e = threadIdx.x; e < entries; e += blockDim.x) s_acc[e] = 0ull;
+  __syncthreads();
+  if (valid) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 3; ++i) {
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const float3 c = jf_node_contrib(I, st, sc, i, j);
-      const int64_t n = 3 * ((int64_t)(st.by + j) * I.nx + st.bx + i);
-      add_fixed(fix + n + 0, c.x);
-      add_fixed(fix + n + 1, c.y);
-      add_fixed(fix + n + 2, c.z);
+      for (int j = 0; j < 3; ++j) {
+        const float3 c = jf_node_contrib(I, st, sc, i, j);
+        unsigned long long* t = s_acc + 3 * ((st.by + j - y0) * W + (st.bx + i - x0));
+        atomicAdd(t + 0, (unsigned long long)__float2ll_rn(c.x * kFix));
+        atomicAdd(t + 1, (unsigned long long)__float2ll_rn(c.y * kFix));
+        atomicAdd(t + 2, (unsigned long long)__float2ll_rn(c.z * kFix));
+      }
     }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < entries; e += blockDim.x) {
+    const unsigned long long v = s_acc[e];
+    if (v == 0ull) continue;
+    const int node = e / 3, comp = e - 3 * node;
+    const int ty = node / W, tx = node - ty * W;
+    atomicAdd(fix + 3 * ((int64_t)(y0 + ty) * I.nx + x0 + tx) + comp, v);
   }
 }
 

@@ -615,7 +615,15 @@ __global__ void sort_keys_kernel(const JfInst* __restrict__ inst, const float4* 
     }
   }
   keys[g] = key;
-  rank[g] = atomicAdd(counts + (int64_t)m * stride + key, 1);
+  // lanes of the warp with the same cell take one atomic between them (lattice
+  // neighbours share cells); each gets its rank from the group's base
+  const unsigned group = __match_any_sync(__activemask(), key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(group) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counts + (int64_t)m * stride + key, __popc(group));
+  base = __shfl_sync(group, base, leader);
+  rank[g] = base + __popc(group & ((1u << lane) - 1u));
   if (mt > 0 && key < cells && I.ny <= kMaxBandRows) atomicAdd(solid + m * kMaxBandRows + key / I.nx, 1);
 }
 

@@ -664,6 +664,9 @@ def run_ours(args):
                            "path": "batched"},
                 "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": gpu_launches,
                 "nonfinite_instances": int(np.count_nonzero(flags)),
+                # allocated slots (live and dead) x substeps / time: the count the
+                # reference's published per-generation rates use
+                "value_slots": M * args.slots * world * S * K / (ms_max / 1e3),
                 "fwd_bwd_over_fwd": extras.get("differentiable", {}).get("fwd_bwd_over_fwd")}
         line.update(extras)
         print(json.dumps(line), flush=True)

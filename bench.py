@@ -529,7 +529,7 @@ def run_ours(args):
     barrier()
     ms = ev0.elapsed_time(ev1)
     # the state the timed steps ended in, for the plain path's comparison run
-    snapshot = None if args.no_extras else (
+    snapshot = None if (args.no_extras or world > 1) else (
         [engine.read(m) for m in range(M)], engine.get_params(), float(engine.time))
     kt = engine.kernel_timing()
     engine.set_kernel_timing(False)
@@ -557,6 +557,8 @@ def run_ours(args):
                 "sort_ms": kt["sort_ms"], "sort_launches": kt["sort_launches"]}
 
     extras = {}
+    if world > 1 and args.gpus != world:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE {world}")
     if not args.no_extras:
         # the same engine and state, (sort, chunk) pairs replayed from CUDA graphs
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -600,6 +602,7 @@ def run_ours(args):
             from jellyfih_b200.shard import gather_rows
             extras["e2e"]["gathered_results"] = int(gather_rows(res).shape[0])
 
+    if not args.no_extras and world == 1:
         # plain per-instance launch path (the batched / plain ratio): on the
         # state the batched timed steps ended in, and from the loaded inputs
         def time_plain(setup, P=50):
@@ -709,6 +712,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* set per
+        # rank); under torchrun the ranks already exist
+        from jellyfih_b200.launch import spawn_ranks
+        return spawn_ranks(args.gpus, os.path.abspath(__file__), sys.argv[1:])
     if args.grad_only:
         return run_grad_only(args)
     if args.render_only:

@@ -70,8 +70,10 @@ typedef struct {
  * contraction 0.2, frequency multiplier 1.0, payload density 2.5). */
 int jf_create(const jf_config* cfg, jf_engine** out);
 int jf_destroy(jf_engine* e);
-/* Message of the engine's last failure; with e == NULL, of the last failed
- * call made without a handle (jf_create, jf_substep_noalloc). */
+/* Message of the engine's last failure; with e == NULL, of the calling
+ * thread's last failed call made without a handle (jf_create,
+ * jf_substep_noalloc).  The pointer stays valid until that engine's, or that
+ * thread's, next failure. */
 const char* jf_last_error(const jf_engine* e);
 const char* jf_version(void);
 
@@ -263,11 +265,16 @@ int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset);
  * x, v, fiber must be 8-byte and C, F 16-byte aligned.  The grid scratch is a
  * file-scope device array of JF_NOALLOC_MAX_NODES float4 nodes (512 KiB) that
  * every GPU loading the library holds until exit; larger grids are rejected
- * with JF_ERR_UNSUPPORTED.  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress) with that device current, so make that
- * first call before any stream capture.  All calls share the array and each
- * call clears the nodes it uses; calls that overlap on the GPU race.  Work is
- * queued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+ * with JF_ERR_UNSUPPORTED.  Every call looks the array's address up
+ * (cudaGetSymbolAddress, which allocates nothing) in the CUDA context current
+ * on the calling thread, so a device reset or another context on the same
+ * device is followed; the first call on a device may load the library's device
+ * code, so make that first call before any stream capture.  All calls share
+ * the array and each call clears the nodes it uses; calls that overlap on the
+ * GPU race.  A state that turns NaN or Inf is not reported by this entry point
+ * (the engine's jf_error_flags do not see it): check the outputs where that
+ * matters.  Work is queued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream). */
 int jf_substep_noalloc(int32_t n, int32_t n_grid, int32_t n_grid_y, float domain_height, double dt,
                        float sim_time, float actuation, float contraction, float freq,
                        float payload_density, float* x, float* v, float* C, float* F,

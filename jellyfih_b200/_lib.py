@@ -24,6 +24,7 @@ JF_FLAG_AXISYM = 4
 JF_VORT_RDBU = 0
 JF_VORT_HUESHIFT = 1
 JF_VORT_WHITE = 2
+JF_NOALLOC_MAX_NODES = 32768
 
 
 class JfInstanceDesc(ctypes.Structure):

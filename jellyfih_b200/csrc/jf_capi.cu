@@ -4,7 +4,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -16,8 +15,9 @@ int jf_batched_max_active_clusters(jf_engine* e, int cluster, int* out);
 
 namespace {
 
-std::mutex g_err_mu;
-std::string g_create_err;  // message of the last failed call without a handle
+// message of the last failed call without a handle, per host thread, so that
+// the pointer jf_last_error(NULL) returns stays valid while other threads fail
+thread_local std::string g_create_err;
 
 constexpr int kHaloRows = 4;  // batched window rows beyond the band (1 below, 3 above)
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -201,10 +201,7 @@ cudaError_t collect_timing(jf_engine* e) {
 
 }  // namespace
 
-void jf_set_global_error(const std::string& msg) {
-  std::lock_guard<std::mutex> lk(g_err_mu);
-  g_create_err = msg;
-}
+void jf_set_global_error(const std::string& msg) { g_create_err = msg; }
 
 static cudaEvent_t pool_event(jf_engine* e) {
   if (!e->event_pool.empty()) {
@@ -237,7 +234,6 @@ const char* jf_version(void) { return "jellyfih-b200 0.1"; }
 
 const char* jf_last_error(const jf_engine* e) {
   if (e) return e->err.c_str();
-  std::lock_guard<std::mutex> lk(g_err_mu);
   return g_create_err.c_str();
 }
 

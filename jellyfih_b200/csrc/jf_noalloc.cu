@@ -13,7 +13,6 @@
 // All calls share it and it keeps the last call's contents, so each call
 // clears the nodes it uses first, and calls whose work overlaps on the GPU
 // (different streams, or different host threads on one device) race on it.
-#include <mutex>
 #include <string>
 
 #include "jf_engine.h"
@@ -22,12 +21,8 @@ namespace {
 
 constexpr int kMaxNodes = JF_NOALLOC_MAX_NODES;
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) float4 g_noalloc_grid[kMaxNodes];
-
-std::mutex g_mu;
-float4* g_grid_addr[kMaxDevices] = {};  // device address of g_noalloc_grid, per device
 
 int fail(int code, const std::string& msg) {
   jf_set_global_error(msg);
@@ -95,20 +90,15 @@ __global__ void noalloc_g2p(JfInst I, int n, float2* __restrict__ x, float2* __r
   C[k] = Ck;
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress); nullptr on failure.
-float4* scratch_on_current_device(int* dev_out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-  *dev_out = dev;
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_grid_addr[dev]) {
-    float4* ptr = nullptr;
-    const cudaError_t err = cudaGetSymbolAddress((void**)&ptr, g_noalloc_grid);
-    if (err != cudaSuccess) return nullptr;
-    g_grid_addr[dev] = ptr;
-  }
-  return g_grid_addr[dev];
+// Device address of the scratch array in the context current on this thread
+// (cudaGetSymbolAddress; nullptr on failure).  It is looked up on every call,
+// not cached: an address belongs to the context it was taken in, and after a
+// cudaDeviceReset, or with another context made current on the same device,
+// a cached address would point at memory that is no longer the array.
+float4* scratch_in_current_context() {
+  float4* ptr = nullptr;
+  if (cudaGetSymbolAddress((void**)&ptr, g_noalloc_grid) != cudaSuccess) return nullptr;
+  return ptr;
 }
 
 bool aligned(const void* p, size_t a) { return ((uintptr_t)p % a) == 0; }
@@ -131,8 +121,7 @@ extern "C" int jf_substep_noalloc(int32_t n, int32_t n_grid, int32_t n_grid_y, f
     return fail(JF_ERR_INVALID, "jf_substep_noalloc: x, v, C, F, material and Jp are required");
   if (!aligned(x, 8) || !aligned(v, 8) || !aligned(C, 16) || !aligned(F, 16) || !aligned(fiber, 8))
     return fail(JF_ERR_INVALID, "jf_substep_noalloc: x, v, fiber need 8-byte and C, F 16-byte alignment");
-  int dev = -1;
-  float4* grid = scratch_on_current_device(&dev);
+  float4* grid = scratch_in_current_context();
   if (!grid) return fail(JF_ERR_CUDA, "jf_substep_noalloc: scratch array unavailable on this device");
 
   const double dx_d = 1.0 / n_grid;

@@ -2,7 +2,7 @@
 
 Usage (needs the reference checkout, so it runs only where that exists):
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <path of a reference checkout>
 
 Each case runs in a fresh subprocess because mpm_sim.py reads its JELLY_* env
 vars and allocates its fields at import (mpm_sim.py:11-17,86-142).  The
@@ -308,7 +308,9 @@ def _run_case(case, reference):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("JELLYFIH_REFERENCE"),
+                    required="JELLYFIH_REFERENCE" not in os.environ,
+                    help="checkout of the reference (or set JELLYFIH_REFERENCE)")
     ap.add_argument("--case", default=None)
     args = ap.parse_args()
     if args.case:

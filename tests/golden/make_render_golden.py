@@ -2,7 +2,7 @@
 
 Usage (needs the reference checkout, so it runs only where that exists):
 
-    python tests/golden/make_render_golden.py --reference /root/reference
+    python tests/golden/make_render_golden.py --reference <path of a reference checkout>
 
 The reference's render kernels (mpm_sim.py:343-712: clear_frame_buffer,
 render_frame_abyss, tone_map_and_encode, clear_frame_buffer_white,
@@ -205,7 +205,9 @@ def _run_case(case, reference):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("JELLYFIH_REFERENCE"),
+                    required="JELLYFIH_REFERENCE" not in os.environ,
+                    help="checkout of the reference (or set JELLYFIH_REFERENCE)")
     ap.add_argument("--case", default=None)
     args = ap.parse_args()
     if args.case:

@@ -32,23 +32,31 @@ def _norm_close(a, b, rtol, what):
     assert err <= rtol * max(scale, 1e-30), f"{what}: max|diff| {err:.3e} > {rtol} * {scale:.3e}"
 
 
-def test_noalloc_matches_engine_on_two_calls():
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
+FIELDS = ("x", "v", "C", "F", "material", "Jp", "glow", "fiber")
+
+
+def _run_two_calls(n, ny, domain_h, genome_seed, with_fiber_glow, spawn=None):
+    """Two consecutive jf_substep_noalloc calls against one plain-engine
+    substep each, from a state the engine evolved for 300 substeps.  Without
+    fiber and glow the tank's muscle is turned into jelly (a NULL fiber means
+    (0, 1), which only muscle reads) and the glow buffer must come back
+    untouched."""
     from jellyfih_b200 import Engine, InstanceSpec, _lib, build, tank
     build.build()
     lib = _lib.load()
     torch.cuda.set_device(0)
 
-    genome = tank.uniform_genomes(1, 77)[0]
-    n = 80000
-    pos, mat, fib, st = tank.fill_tank(genome, n, jitter=0.25, seed=77)
+    genome = tank.uniform_genomes(1, genome_seed)[0]
+    kw = {} if spawn is None else {"spawn_offset": spawn}
+    pos, mat, fib, st = tank.fill_tank(genome, n, domain_height=domain_h, jitter=0.25, seed=genome_seed, **kw)
+    if not with_fiber_glow:
+        mat = np.where(mat == 3, 1, mat).astype(np.int32)
     contraction, freq = tank.timing_params(genome)
     live = mat >= 0
     act, pdens, dt = 650.0, 3.0, 2e-5
 
     # a naturally evolved state: 300 substeps of the engine from the loaded tank
-    eng = Engine([InstanceSpec(n)], path="plain", glow=True)
+    eng = Engine([InstanceSpec(n, 128, ny, domain_h)], path="plain", glow=True)
     eng.load(0, pos, mat, fib)
     eng.set_params(actuation=[act], contraction=[contraction], freq=[freq], payload_density=[pdens])
     eng.time = 0.0
@@ -57,18 +65,20 @@ def test_noalloc_matches_engine_on_two_calls():
     t0 = eng.time
 
     dev = torch.device("cuda", 0)
-    bufs = {k: torch.from_numpy(np.ascontiguousarray(s0[k])).to(dev)
-            for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber")}
+    bufs = {k: torch.from_numpy(np.ascontiguousarray(s0[k])).to(dev) for k in FIELDS}
+    glow0 = s0["glow"].copy()
     stream = torch.cuda.current_stream(dev)
     t = t0
     for call in range(2):
         if call > 0:  # both paths start this call from the first call's output
             eng.write(0, x=got["x"], v=got["v"], C=got["C"], F=got["F"], Jp=got["Jp"],
-                      glow=got["glow"])
-        rc = lib.jf_substep_noalloc(
-            n, 128, 128, 1.0, dt, float(t), act, contraction, freq, pdens,
-            *[bufs[k].data_ptr() for k in ("x", "v", "C", "F", "material", "Jp", "glow", "fiber")],
-            stream.cuda_stream)
+                      glow=got["glow"] if with_fiber_glow else None)
+        ptrs = [bufs[k].data_ptr() for k in FIELDS]
+        if not with_fiber_glow:
+            ptrs[FIELDS.index("glow")] = None
+            ptrs[FIELDS.index("fiber")] = None
+        rc = lib.jf_substep_noalloc(n, 128, ny, domain_h, dt, float(t), act, contraction, freq, pdens,
+                                    *ptrs, stream.cuda_stream)
         assert rc == 0, lib.jf_last_error(None)
         t = np.float32(t + np.float32(dt))
         eng.step(1)
@@ -77,11 +87,30 @@ def test_noalloc_matches_engine_on_two_calls():
         got = {k: bufs[k].cpu().numpy() for k in ("x", "v", "C", "F", "Jp", "glow")}
         tol_x = 4 * np.spacing(np.float32(1.0))
         assert np.abs(got["x"][live].astype(np.float64) - ref["x"][live]).max() <= tol_x, call
-        for k in ("v", "C", "F", "Jp", "glow"):
+        for k in ("v", "C", "F", "Jp"):
             _norm_close(got[k][live], ref[k][live], FIELD_RTOL, f"call {call} {k}")
+        if with_fiber_glow:
+            _norm_close(got["glow"][live], ref["glow"][live], FIELD_RTOL, f"call {call} glow")
+        else:
+            assert np.array_equal(got["glow"], glow0), "glow changed although the call passed NULL"
         assert np.array_equal(got["x"][~live], ref["x"][~live])
     assert eng.time == t
     eng.close()
+
+
+@pytest.mark.parametrize("case", ["square_fiber_glow", "tall_at_node_cap", "no_fiber_no_glow"])
+def test_noalloc_matches_engine_on_two_calls(case):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import _lib, tank
+    if case == "square_fiber_glow":
+        _run_two_calls(80000, 128, 1.0, 77, True)
+    elif case == "tall_at_node_cap":
+        # 128 x 256 = JF_NOALLOC_MAX_NODES: the largest grid the scratch array holds
+        assert 128 * 256 == _lib.JF_NOALLOC_MAX_NODES
+        _run_two_calls(160000, 256, 2.0, 78, True, spawn=tank.TALL_SPAWN)
+    else:
+        _run_two_calls(80000, 128, 1.0, 79, False)
 
 
 def test_noalloc_rejects_oversized_grid_and_bad_arguments():

@@ -27,8 +27,11 @@ extern "C" {
 #define JF_ERR_INVALID 1      /* bad argument, shape or state */
 #define JF_ERR_CUDA 2         /* a CUDA call failed */
 #define JF_ERR_NONFINITE 3    /* a particle state became NaN/Inf: returned, after their outputs
-                                 are written, by jf_sync, jf_run_headless and jf_run_episode while
-                                 an instance's flag is set (jf_error_flags / jf_clear_error_flags) */
+                                 are written, by jf_sync, jf_run_headless, jf_run_episode,
+                                 jf_grad_forward and jf_grad_backward while an instance's flag is
+                                 set (jf_error_flags / jf_clear_error_flags); the gradient path
+                                 also flags P2G contributions too large for its fixed-point sums
+                                 and non-finite adjoint states */
 #define JF_ERR_UNSUPPORTED 4  /* configuration outside what the chosen path supports */
 
 #define JF_PATH_PLAIN 0       /* one instance per launch sequence (reference structure) */
@@ -160,8 +163,13 @@ int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, cons
  * instance_freq (host arrays, NULL to skip; the refractory fraction is
  * 1 - contraction, so its gradient is minus the contraction's), and
  * jf_grad_positions the gradient w.r.t. instance m's initial positions in slot
- * order ([n_slots][2]).  The reference engine has no gradients; this replaces
- * nothing in it.  The engine is left at the rollout's final state. */
+ * order ([n_slots][2]).  The waveform's drop from 1 to 0 when the phase
+ * reaches the contraction fraction (mpm_sim.py:176-180) is differentiated as
+ * the boundary term of the time integral: each drop inside the rollout adds
+ * actuation * g / (freq * dt) to d/d contraction and minus that times the
+ * drop's time to d/d freq, g being d loss / d pressure at the drop.  The
+ * reference engine has no gradients; this replaces nothing in it.  The engine
+ * is left at the rollout's final state. */
 int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss);
 int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, double* d_freq);
 int jf_grad_positions(jf_engine* e, int32_t m, float* dx0);

@@ -64,21 +64,25 @@ def refine_timing_genes(engine, genomes, positions, materials, fibers, steps, it
 
     Each iteration moves each gene by step_frac of its range in the direction
     that raises the payload's displacement, clipped to the gene bounds
-    (evolve.py:55-62).  Returns the refined genomes and the displacement
-    before every step.
+    (evolve.py:55-62).  An instance whose rollout or adjoint went non-finite
+    (the engine's error flags) keeps its genes for that iteration.  Returns
+    the refined genomes and the displacement before every step.
     """
     g = np.array(genomes, dtype=np.float64, copy=True)
     M = len(g)
     pos = torch.as_tensor(np.stack(positions), dtype=torch.float32)
     history = []
     for _ in range(iterations):
+        engine.clear_error_flags()
         c = torch.tensor(np.clip(g[:, 9], 0.05, 0.60), dtype=torch.float64, requires_grad=True)
         f = torch.tensor(np.clip(g[:, 10], 0.5, 2.0), dtype=torch.float64, requires_grad=True)
         a = torch.full((M,), actuation, dtype=torch.float64)
         disp = rollout_displacement(engine, a, c, f, pos, materials, fibers, steps, checkpoint_every)
         disp.sum().backward()
         history.append(disp.detach().numpy().copy())
+        ok = engine.error_flags() == 0
         for k, grad in ((9, c.grad), (10, f.grad)):
             span = GENOME_UPPER[k] - GENOME_LOWER[k]
-            g[:, k] = np.clip(g[:, k] + step_frac * span * np.sign(grad.numpy()), GENOME_LOWER[k], GENOME_UPPER[k])
+            step = np.where(ok, step_frac * span * np.sign(np.nan_to_num(grad.numpy())), 0.0)
+            g[:, k] = np.clip(g[:, k] + step, GENOME_LOWER[k], GENOME_UPPER[k])
     return g, history

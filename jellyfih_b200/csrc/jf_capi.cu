@@ -806,7 +806,9 @@ int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, doubl
     if (loss) loss[m] = fin - init[m];
   }
   e->sorted = false;
-  return JF_OK;
+  std::vector<int32_t> flags;
+  if ((rc = read_flags_and_sync(e, flags))) return rc;
+  return nonfinite_status(e, flags);
 }
 
 int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, double* d_freq) {
@@ -821,7 +823,9 @@ int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, d
     if (d_contraction) d_contraction[m] = g[3 * (size_t)m + 1];
     if (d_freq) d_freq[m] = g[3 * (size_t)m + 2];
   }
-  return JF_OK;
+  std::vector<int32_t> flags;
+  if ((rc = read_flags_and_sync(e, flags))) return rc;
+  return nonfinite_status(e, flags);
 }
 
 int jf_grad_positions(jf_engine* e, int32_t m, float* dx0) {

@@ -173,6 +173,29 @@ __device__ __forceinline__ bool jf_stencil(const JfInst& I, float2 x, JfStencil&
   return true;
 }
 
+// jf_stencil with every operation rounded on its own, as the reference's FP32
+// arithmetic rounds it (the base cast, fx and the weights; no fused
+// multiply-adds).  The differentiable rollout's deterministic forward and its
+// adjoints use it, so that their stencils match the oracle's bit for bit.
+__device__ __forceinline__ bool jf_stencil_strict(const JfInst& I, float2 x, JfStencil& st) {
+  const float X = __fmul_rn(x.x, I.inv_dx), Y = __fmul_rn(x.y, I.inv_dx);
+  st.bx = (int)__fsub_rn(X, 0.5f);
+  st.by = (int)__fsub_rn(Y, 0.5f);
+  if (st.bx < 0 || st.by < 0 || st.bx >= I.nx - 2 || st.by >= I.ny - 2) return false;
+  st.fx0 = __fsub_rn(X, (float)st.bx);
+  st.fx1 = __fsub_rn(Y, (float)st.by);
+  const float a0 = __fsub_rn(1.5f, st.fx0), a1 = __fsub_rn(1.5f, st.fx1);
+  const float b0 = __fsub_rn(st.fx0, 1.0f), b1 = __fsub_rn(st.fx1, 1.0f);
+  const float e0 = __fsub_rn(st.fx0, 0.5f), e1 = __fsub_rn(st.fx1, 0.5f);
+  st.wx0 = __fmul_rn(0.5f, __fmul_rn(a0, a0));
+  st.wx1 = __fsub_rn(0.75f, __fmul_rn(b0, b0));
+  st.wx2 = __fmul_rn(0.5f, __fmul_rn(e0, e0));
+  st.wy0 = __fmul_rn(0.5f, __fmul_rn(a1, a1));
+  st.wy1 = __fsub_rn(0.75f, __fmul_rn(b1, b1));
+  st.wy2 = __fmul_rn(0.5f, __fmul_rn(e1, e1));
+  return true;
+}
+
 __device__ __forceinline__ float jf_w(const JfStencil& s, int axis, int k) {
   if (axis == 0) return k == 0 ? s.wx0 : (k == 1 ? s.wx1 : s.wx2);
   return k == 0 ? s.wy0 : (k == 1 ? s.wy1 : s.wy2);
@@ -302,6 +325,18 @@ __device__ __forceinline__ float3 jf_node_contrib(const JfInst& I, const JfStenc
   return make_float3(c0, c1, weight * sc.mass);
 }
 
+// jf_node_contrib with every operation rounded on its own (mpm_sim.py:256-271
+// evaluated as the reference's FP32 code evaluates it).
+__device__ __forceinline__ float3 jf_node_contrib_strict(const JfInst& I, const JfStencil& st,
+                                                         const JfScatter& sc, int i, int j) {
+  const float d0 = __fmul_rn(__fsub_rn((float)i, st.fx0), I.dx);
+  const float d1 = __fmul_rn(__fsub_rn((float)j, st.fx1), I.dx);
+  const float weight = __fmul_rn(jf_w(st, 0, i), jf_w(st, 1, j));
+  const float c0 = __fmul_rn(weight, __fadd_rn(sc.mv0, rdot2(sc.af00, d0, sc.af01, d1)));
+  const float c1 = __fmul_rn(weight, __fadd_rn(sc.mv1, rdot2(sc.af10, d0, sc.af11, d1)));
+  return make_float3(c0, c1, __fmul_rn(weight, sc.mass));
+}
+
 // Grid node update (mpm_sim.py:274-309): normalise by mass, damp in a band of
 // n//20 nodes on all four sides, zero the velocity component pointing into a
 // wall within 3 nodes.  Nodes without mass keep their (zero) momentum.
@@ -368,6 +403,38 @@ __device__ __forceinline__ void jf_g2p_apic(const JfInst& I, const JfStencil& st
   }
   v = make_float2(nv0, nv1);
   C = make_float4(I.c4 * c00, I.c4 * c01, I.c4 * c10, I.c4 * c11);
+}
+
+// The APIC gather of G2P in the reference's own operation order
+// (mpm_sim.py:317-327): nodes i outer, j inner, weight = w_i w_j,
+// new_v += weight g_v and new_C += (4 inv_dx weight) (g_v outer dpos), every
+// operation rounded on its own.  The deterministic forward of the
+// differentiable rollout uses it, so that the rollout reproduces the oracle's
+// arithmetic exactly apart from the order of the P2G sums.
+template <class Gather>
+__device__ __forceinline__ void jf_g2p_apic_nodes(const JfInst& I, const JfStencil& st, float2& v, float4& C,
+                                                  Gather gather) {
+  const float wx[3] = {st.wx0, st.wx1, st.wx2};
+  const float wy[3] = {st.wy0, st.wy1, st.wy2};
+  float nv0 = 0.f, nv1 = 0.f, c00 = 0.f, c01 = 0.f, c10 = 0.f, c11 = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float d0 = __fsub_rn((float)i, st.fx0), d1 = __fsub_rn((float)j, st.fx1);
+      const float2 g = gather(i, j);
+      const float w = __fmul_rn(wx[i], wy[j]);
+      nv0 = __fadd_rn(nv0, __fmul_rn(w, g.x));
+      nv1 = __fadd_rn(nv1, __fmul_rn(w, g.y));
+      const float k = __fmul_rn(I.c4, w);
+      c00 = __fadd_rn(c00, __fmul_rn(k, __fmul_rn(g.x, d0)));
+      c01 = __fadd_rn(c01, __fmul_rn(k, __fmul_rn(g.x, d1)));
+      c10 = __fadd_rn(c10, __fmul_rn(k, __fmul_rn(g.y, d0)));
+      c11 = __fadd_rn(c11, __fmul_rn(k, __fmul_rn(g.y, d1)));
+    }
+  }
+  v = make_float2(nv0, nv1);
+  C = make_float4(c00, c01, c10, c11);
 }
 
 // Gravity, advection and the wall clamp of every live particle

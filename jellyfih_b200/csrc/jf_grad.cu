@@ -15,9 +15,28 @@
 // (SVD, plasticity, stress) is differentiated with four-tangent dual numbers
 // (jf_dual.cuh); everything else is written out by hand.  Integer cell bases,
 // clamps at their bounds and boundary-zeroed grid components carry no
-// gradient, as in an autodiff of the same code.  The waveform's drop from 1
-// to 0 at phase == contraction contributes no gradient (a discrete adjoint
-// does not see the jump).
+// gradient, as in an autodiff of the same code.
+//
+// The waveform drops from 1 to 0 when the phase reaches the contraction
+// fraction (mpm_sim.py:176-180).  A discrete adjoint does not see that jump
+// (nor would Taichi's autodiff), but moving the contraction fraction or the
+// frequency moves the instant of the drop, and the loss moves with it.  The
+// backward therefore records dL/dpressure of every substep and adds, for every
+// drop inside the rollout, the boundary term of the time integral:
+// dL/dc += A g* / (f dt) and dL/df -= A g* t* / (f^2 dt) (t* the instant of
+// the drop, g* dL/dpressure there, interpolated between the substeps around
+// it; a(c-) = 1).
+//
+// Non-finite states: G2P flags an instance whose position or velocity is NaN
+// or Inf, and P2G flags a contribution too large for the fixed-point sums
+// (|value| >= 64, far beyond any physical momentum or mass of a particle), and
+// adds zero for it; the adjoint flags non-finite adjoint states.  The flags
+// are the engine's non-finite flags (jf_error_flags).
+
+// Every operation of the deterministic forward is rounded on its own (the
+// stencil, the node contributions and the G2P gather in the reference's node
+// order), so that, apart from the order-free fixed-point P2G sums, it performs
+// the reference's FP32 arithmetic exactly.
 #include <vector>
 
 #include "jf_dual.cuh"
@@ -47,11 +66,27 @@ struct GradArgs {
   unsigned long long* fix;     // 3 per node: momentum x, momentum y, mass (fixed point)
   float2* u;                   // updated grid velocity
   float4* pmv;                 // if set: (momentum x, momentum y, mass) per node, kept for the adjoint
+  int32_t* err;                // per-instance non-finite flags
   float t;
 };
 
-__device__ __forceinline__ void add_fixed(unsigned long long* p, float v) {
-  atomicAdd(p, (unsigned long long)__float2ll_rn(v * kFix));
+// Largest contribution the fixed-point sums take: |v| < 64 keeps v * 2^44
+// below 2^50, so 8,192 contributions to one node cannot overflow 2^63.
+constexpr float kFixMax = 64.0f;
+
+// v in 2^-44 fixed point; a non-finite or out-of-range v sets the instance's
+// flag (bit 2) and contributes zero.
+__device__ __forceinline__ unsigned long long to_fixed(float v, int32_t* flag) {
+  if (!(fabsf(v) < kFixMax)) {
+    atomicOr(flag, 2);
+    return 0ull;
+  }
+  return (unsigned long long)__float2ll_rn(v * kFix);
+}
+
+__device__ __forceinline__ void add_fixed(unsigned long long* p, float v, int32_t* flag) {
+  const unsigned long long q = to_fixed(v, flag);
+  if (q) atomicAdd(p, q);
 }
 __device__ __forceinline__ float from_fixed(unsigned long long v) {
   return (float)((double)(long long)v * kFixInv);
@@ -92,7 +127,7 @@ __global__ void __launch_bounds__(kT) gf_p2g(GradArgs a) {
   if (k < I.n_slots) {
     const int mt = a.mat[g];
     const float4 xv = mt >= 0 ? a.s.xv[g] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (mt >= 0 && jf_stencil(I, make_float2(xv.x, xv.y), st)) {
+    if (mt >= 0 && jf_stencil_strict(I, make_float2(xv.x, xv.y), st)) {
       float4 F = a.s.F[g];
       float jp = (mt == 2) ? a.Jp[g] : 1.0f;
       const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
@@ -127,11 +162,11 @@ __global__ void __launch_bounds__(kT) gf_p2g(GradArgs a) {
     for (int i = 0; i < 3; ++i) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const float3 c = jf_node_contrib(I, st, sc, i, j);
+        const float3 c = jf_node_contrib_strict(I, st, sc, i, j);
         const int64_t n = 3 * ((int64_t)(st.by + j) * I.nx + st.bx + i);
-        add_fixed(fix + n + 0, c.x);
-        add_fixed(fix + n + 1, c.y);
-        add_fixed(fix + n + 2, c.z);
+        add_fixed(fix + n + 0, c.x, a.err + m);
+        add_fixed(fix + n + 1, c.y, a.err + m);
+        add_fixed(fix + n + 2, c.z, a.err + m);
       }
     }
     return;
@@ -144,11 +179,11 @@ __global__ void __launch_bounds__(kT) gf_p2g(GradArgs a) {
     for (int i = 0; i < 3; ++i) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const float3 c = jf_node_contrib(I, st, sc, i, j);
+        const float3 c = jf_node_contrib_strict(I, st, sc, i, j);
         unsigned long long* t = s_acc + 3 * ((st.by + j - y0) * W + (st.bx + i - x0));
-        atomicAdd(t + 0, (unsigned long long)__float2ll_rn(c.x * kFix));
-        atomicAdd(t + 1, (unsigned long long)__float2ll_rn(c.y * kFix));
-        atomicAdd(t + 2, (unsigned long long)__float2ll_rn(c.z * kFix));
+        atomicAdd(t + 0, to_fixed(c.x, a.err + m));
+        atomicAdd(t + 1, to_fixed(c.y, a.err + m));
+        atomicAdd(t + 2, to_fixed(c.z, a.err + m));
       }
     }
   }
@@ -191,7 +226,12 @@ __global__ void gf_g2p(GradArgs a) {
   float4 C = a.s.C[g];
   const float2* u = a.u + I.g_off;
   const int nx = I.nx;
-  jf_g2p_particle(I, x, v, C, [&](int ni, int nj) { return u[nj * nx + ni]; });
+  JfStencil st;
+  if (jf_stencil_strict(I, x, st)) {
+    jf_g2p_apic_nodes(I, st, v, C, [&](int i, int j) { return u[(st.by + j) * nx + st.bx + i]; });
+  }
+  jf_g2p_advect(I, x, v);
+  if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
   a.o.xv[g] = make_float4(x.x, x.y, v.x, v.y);
   a.o.C[g] = C;
 }
@@ -206,6 +246,7 @@ struct AdjArgs {
   float2* xtmp;        // G2P part of the position adjoint
   float2* vtmp;        // velocity adjoint of particles outside the stencil range
   double* gparam;      // M x 3: d/d actuation, d/d contraction, d/d freq
+  double* dLdp;        // M: d L / d pressure of this substep, per instance
 };
 
 __device__ __forceinline__ float wd(int k, float f) {  // d W_k / d f
@@ -229,13 +270,13 @@ __global__ void ad_g2p(AdjArgs A) {
   const float4 lxv = A.lxv[g];
   const float4 Cb = A.lC[g];
   JfStencil st;
-  const bool inr = jf_stencil(I, x, st);
+  const bool inr = jf_stencil_strict(I, x, st);
   const float2* u = a.u + I.g_off;
   const int nx = I.nx;
   float2 vn = v;
   if (inr) {
     float4 Cn;
-    jf_g2p_apic(I, st, vn, Cn, [&](int i, int j) { return u[(st.by + j) * nx + st.bx + i]; });
+    jf_g2p_apic_nodes(I, st, vn, Cn, [&](int i, int j) { return u[(st.by + j) * nx + st.bx + i]; });
   }
   vn.y = vn.y - I.dtg;
   const float xpp0 = __fadd_rn(x.x, __fmul_rn(I.dt, vn.x));
@@ -338,7 +379,7 @@ __global__ void ad_p2g(AdjArgs A) {
       const float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
       JfStencil st;
       const float2 xt = A.xtmp[g];
-      if (!jf_stencil(I, x, st)) {
+      if (!jf_stencil_strict(I, x, st)) {
         A.lxv[g] = make_float4(xt.x, xt.y, A.vtmp[g].x, A.vtmp[g].y);
         // C and F pass through unchanged outside the stencil range
       } else {
@@ -435,9 +476,14 @@ __global__ void ad_p2g(AdjArgs A) {
         const float Cb01 = mass * Ab01 + dt * (Fsb[0] * F.z + Fsb[1] * F.w);
         const float Cb10 = mass * Ab10 + dt * (Fsb[2] * F.x + Fsb[3] * F.y);
         const float Cb11 = mass * Ab11 + dt * (Fsb[2] * F.z + Fsb[3] * F.w);
-        A.lxv[g] = make_float4(xt.x + I.inv_dx * xb0 - xa0, xt.y + I.inv_dx * xb1 - xa1, mass * vb0, mass * vb1);
+        const float4 lx = make_float4(xt.x + I.inv_dx * xb0 - xa0, xt.y + I.inv_dx * xb1 - xa1, mass * vb0,
+                                      mass * vb1);
+        A.lxv[g] = lx;
         A.lC[g] = make_float4(Cb00, Cb01, Cb10, Cb11);
         A.lF[g] = make_float4(Fb00, Fb01, Fb10, Fb11);
+        const float chk = ((lx.x + lx.y) + (lx.z + lx.w)) + ((Cb00 + Cb01) + (Cb10 + Cb11)) +
+                          ((Fb00 + Fb01) + (Fb10 + Fb11));
+        if (!isfinite(chk)) atomicOr(a.err + m, 4);
       }
     }
   }
@@ -454,6 +500,7 @@ __global__ void ad_p2g(AdjArgs A) {
       atomicAdd(A.gparam + 3 * m + 0, tot * s_fac[0]);
       atomicAdd(A.gparam + 3 * m + 1, tot * s_fac[1]);
       atomicAdd(A.gparam + 3 * m + 2, tot * s_fac[2]);
+      atomicAdd(A.dLdp + m, tot);
     }
   }
 }
@@ -507,6 +554,8 @@ struct JfGrad {
   float4* fin = nullptr;    // final state (3 arrays)
   float* fin_Jp = nullptr;  // final Jp (the backward's recompute updates Jp in place)
   double* gparam = nullptr;
+  double* dLdp = nullptr;   // steps x M: d L / d pressure per substep and instance
+  size_t dLdp_cap = 0;
   int32_t* body_mode = nullptr;
   double* inv_n = nullptr;
   std::vector<double> loss;
@@ -519,6 +568,7 @@ void jf_grad_free(jf_engine* e) {
   cudaFree(G->fix); cudaFree(G->u); cudaFree(G->ubar); cudaFree(G->pmbar);
   cudaFree(G->lxv); cudaFree(G->lC); cudaFree(G->lF); cudaFree(G->xtmp); cudaFree(G->vtmp);
   cudaFree(G->ck); cudaFree(G->seg); cudaFree(G->useg); cudaFree(G->pmseg); cudaFree(G->fin); cudaFree(G->fin_Jp); cudaFree(G->gparam);
+  cudaFree(G->dLdp);
   cudaFree(G->body_mode); cudaFree(G->inv_n);
   delete G;
   e->grad = nullptr;
@@ -538,6 +588,7 @@ static GradArgs grad_args(jf_engine* e, GradState s, float t) {
   a.fix = G->fix;
   a.u = G->u;
   a.pmv = nullptr;
+  a.err = e->d_err;
   a.t = t;
   return a;
 }
@@ -606,18 +657,12 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
     if ((err = alloc_n(&G->ck, 3 * slots * n_ck)) != cudaSuccess) return err;
     G->n_ck = n_ck;
   }
-  if (G->seg_cap < (size_t)K) {
-    cudaFree(G->seg);
-    cudaFree(G->useg);
-    cudaFree(G->pmseg);
-    G->seg = nullptr;
-    G->useg = nullptr;
-    G->pmseg = nullptr;
-    G->seg_cap = 0;
-    if ((err = alloc_n(&G->seg, 3 * slots * (size_t)K)) != cudaSuccess) return err;
-    if ((err = alloc_n(&G->useg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
-    if ((err = alloc_n(&G->pmseg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
-    G->seg_cap = (size_t)K;
+  if (G->dLdp_cap < (size_t)steps * e->M) {
+    cudaFree(G->dLdp);
+    G->dLdp = nullptr;
+    G->dLdp_cap = 0;
+    if ((err = alloc_n(&G->dLdp, (size_t)steps * e->M)) != cudaSuccess) return err;
+    G->dLdp_cap = (size_t)steps * e->M;
   }
   if ((err = cudaMemcpyAsync(G->body_mode, body_mode, sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream)))
     return err;
@@ -647,6 +692,45 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
   return cudaSuccess;
 }
 
+// Phase of the waveform at time t in FP32, as jf_activation computes it
+// (mpm_sim.py:173-174).
+static float waveform_phase(float freq, float t) {
+  volatile float period = 1.0f / (1.0f * freq);
+  volatile float q = floorf(t / period);
+  volatile float pq = period * q;
+  volatile float r = t - pq;
+  volatile float phase = r / period;
+  return phase;
+}
+
+// Boundary terms of the waveform's drop from 1 to 0 at phase == contraction
+// (mpm_sim.py:176-180): for every drop between substeps n - 1 and n of the
+// rollout, at the instant t* where the phase, advancing by f per unit time,
+// reaches c, d L / d c += A g* / (f dt) and d L / d f -= A g* t* / (f dt), with
+// g* = d L / d pressure interpolated between the two substeps (the rollout's
+// pressure at substep n is A a(phase(t_n)), and a(c-) = 1).
+static void add_waveform_drop_terms(const jf_engine* e, const std::vector<float>& ts,
+                                    const std::vector<double>& dLdp, double* gparam) {
+  const int64_t steps = (int64_t)ts.size() - 1;
+  for (int m = 0; m < e->M; ++m) {
+    const JfParams& P = e->params[m];
+    const double A = P.actuation, c = P.contraction, f = P.freq;
+    if (!(f > 0.0) || !(c > 0.0) || A == 0.0) continue;
+    float prev = waveform_phase(P.freq, ts[0]);
+    for (int64_t n = 1; n < steps; ++n) {
+      const float ph = waveform_phase(P.freq, ts[(size_t)n]);
+      if (prev < P.contraction && !(ph < P.contraction) && ph >= prev) {
+        const double theta = (c - (double)prev) / ((double)ph - (double)prev);
+        const double tstar = (double)ts[(size_t)n - 1] + theta * ((double)ts[(size_t)n] - (double)ts[(size_t)n - 1]);
+        const double g = (1.0 - theta) * dLdp[(size_t)(n - 1) * e->M + m] + theta * dLdp[(size_t)n * e->M + m];
+        gparam[3 * m + 1] += A * g / (f * e->dt);
+        gparam[3 * m + 2] -= A * g * tstar / (f * e->dt);
+      }
+      prev = ph;
+    }
+  }
+}
+
 cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   JfGrad* G = e->grad;
   const size_t slots = (size_t)e->total_slots;
@@ -659,8 +743,24 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   const dim3 gp((e->max_slots + kT - 1) / kT, e->M), gn((e->max_cells + kT - 1) / kT, e->M);
   cudaError_t err = cudaMemsetAsync(G->gparam, 0, sizeof(double) * 3 * e->M, e->stream);
   if (err != cudaSuccess) return err;
+  if ((err = cudaMemsetAsync(G->dLdp, 0, sizeof(double) * (size_t)steps * e->M, e->stream))) return err;
   seed_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, e->p.mat, G->body_mode, G->inv_n, G->lxv, G->lC, G->lF, 1, 1.0f);
   e->launches += 1;
+  // the segment buffers (K pre-step states and grids) are needed only here,
+  // so a forward-only rollout does not hold them
+  if (G->seg_cap < (size_t)K) {
+    cudaFree(G->seg);
+    cudaFree(G->useg);
+    cudaFree(G->pmseg);
+    G->seg = nullptr;
+    G->useg = nullptr;
+    G->pmseg = nullptr;
+    G->seg_cap = 0;
+    if ((err = alloc_n(&G->seg, 3 * slots * (size_t)K)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->useg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->pmseg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+    G->seg_cap = (size_t)K;
+  }
   const GradState work{e->p.xv, e->p.C, e->p.F};
   const int64_t n_seg = (steps + K - 1) / K;
   for (int64_t seg = n_seg - 1; seg >= 0; --seg) {
@@ -689,6 +789,7 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
       A.xtmp = G->xtmp;
       A.vtmp = G->vtmp;
       A.gparam = G->gparam;
+      A.dLdp = G->dLdp + (size_t)(s0 + j) * e->M;
       // the substep's grid as the recompute left it
       A.f.u = G->useg + nodes * j;
       A.f.pmv = G->pmseg + nodes * j;
@@ -709,7 +810,13 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
     return err;
   if ((err = cudaMemcpyAsync(gparam_host, G->gparam, sizeof(double) * 3 * e->M, cudaMemcpyDeviceToHost, e->stream)))
     return err;
-  return cudaStreamSynchronize(e->stream);
+  std::vector<double> dLdp((size_t)steps * e->M);
+  if ((err = cudaMemcpyAsync(dLdp.data(), G->dLdp, sizeof(double) * dLdp.size(), cudaMemcpyDeviceToHost,
+                             e->stream)))
+    return err;
+  if ((err = cudaStreamSynchronize(e->stream))) return err;
+  add_waveform_drop_terms(e, ts, dLdp, gparam_host);
+  return cudaSuccess;
 }
 
 // Position adjoint of the initial state for one instance, in engine order.

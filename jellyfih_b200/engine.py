@@ -230,16 +230,20 @@ class Engine:
 
     # -- differentiable rollout -----------------------------------------------
     def grad_forward(self, steps: int, checkpoint_every: int = 100) -> np.ndarray:
-        """Rollout with checkpoints; returns the (M,) CoM displacement (the loss)."""
+        """Rollout with checkpoints; returns the (M,) CoM displacement (the loss).
+        An instance whose state turned non-finite (or too large for the
+        fixed-point P2G) is recorded as for run_headless: error_flags() names
+        it, and its loss and gradients are not to be used."""
         loss = np.zeros(self.M, np.float64)
-        self._check(self._lib.jf_grad_forward(self._h, int(steps), int(checkpoint_every), _ptr(loss)))
+        self._check_run(self._lib.jf_grad_forward(self._h, int(steps), int(checkpoint_every), _ptr(loss)))
         return loss
 
     def grad_backward(self) -> dict:
-        """d loss / d (actuation, contraction, freq), each (M,)."""
+        """d loss / d (actuation, contraction, freq), each (M,).  Non-finite
+        adjoint states are recorded as in grad_forward."""
         g = {k: np.zeros(self.M, np.float64) for k in ("actuation", "contraction", "freq")}
-        self._check(self._lib.jf_grad_backward(self._h, _ptr(g["actuation"]), _ptr(g["contraction"]),
-                                               _ptr(g["freq"])))
+        self._check_run(self._lib.jf_grad_backward(self._h, _ptr(g["actuation"]), _ptr(g["contraction"]),
+                                                   _ptr(g["freq"])))
         return g
 
     def grad_positions(self, m: int) -> np.ndarray:

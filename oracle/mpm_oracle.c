@@ -65,7 +65,26 @@ typedef struct {
   double freq;         /* instance_freq[m]           mpm_sim.py:125,149 */
   double payload_density; /* instance_payload_density[m] mpm_sim.py:142,147 */
   int32_t axisym;      /* JELLY_AXISYM            mpm_sim.py:17 */
+  int32_t fixed_p2g;   /* not in the reference: sum P2G in 2^-44 fixed point (below) */
 } oracle_inst;
+
+/* Order-free P2G sums (fixed_p2g != 0).  Each momentum / mass contribution is
+ * rounded to the nearest multiple of 2^-44 (an int64; contributions of
+ * magnitude >= 64 count as zero), the node sums are integer sums, whose value
+ * does not depend on the order of the additions, and each sum is converted
+ * back as (REAL)((double)sum * 2^-44) before the grid update.  This is the
+ * accumulation the GPU engine's deterministic forward (the differentiable
+ * rollout) uses; with it the oracle and that forward can be compared over
+ * long rollouts without the summation-order noise of floating-point sums.
+ * The reference itself sums in FP32 (mpm_sim.py:269-270). */
+static const double kFixScale = 17592186044416.0; /* 2^44 */
+
+static uint64_t FN(to_fixed)(REAL v) {
+  if (!(fabs((double)v) < 64.0)) return 0;
+  return (uint64_t)llrint((double)v * kFixScale);
+}
+
+static REAL FN(from_fixed)(uint64_t v) { return (REAL)((double)(int64_t)v * (1.0 / kFixScale)); }
 
 /* Material constants, Python doubles (mpm_sim.py:25-48). */
 static const double E_base = 0.1e4, nu_base = 0.2;
@@ -174,6 +193,8 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
   /* 1. grid clear (:160-165); the axisymmetric stress sums are scratch here */
   memset(gv, 0, sizeof(REAL) * 2 * (size_t)nx * ny);
   memset(gm, 0, sizeof(REAL) * (size_t)nx * ny);
+  uint64_t* gfix = NULL; /* fixed_p2g: momentum x, momentum y, mass per node */
+  if (I->fixed_p2g && !axisym) gfix = (uint64_t*)calloc((size_t)3 * nx * ny, sizeof(uint64_t));
   REAL* gsr = NULL;
   REAL* gsh = NULL;
   if (axisym) {
@@ -298,6 +319,12 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
         REAL c0 = weight * (mv0 + (af00 * d0 + af01 * d1));
         REAL c1 = weight * (mv1 + (af10 * d0 + af11 * d1));
         size_t node = (size_t)(bx + i) * ny + (size_t)(by + j);
+        if (gfix) {
+          gfix[3 * node] += FN(to_fixed)(c0);
+          gfix[3 * node + 1] += FN(to_fixed)(c1);
+          gfix[3 * node + 2] += FN(to_fixed)(weight * mass);
+          continue;
+        }
         gv[2 * node] = gv[2 * node] + c0;
         gv[2 * node + 1] = gv[2 * node + 1] + c1;
         if (axisym) {  /* :264-268 */
@@ -310,6 +337,15 @@ void FN(oracle_substep)(const oracle_inst* I, int64_t n, REAL* x, REAL* v, REAL*
         }
       }
     }
+  }
+
+  if (gfix) {
+    for (size_t node = 0; node < (size_t)nx * ny; ++node) {
+      gv[2 * node] = FN(from_fixed)(gfix[3 * node]);
+      gv[2 * node + 1] = FN(from_fixed)(gfix[3 * node + 1]);
+      gm[node] = FN(from_fixed)(gfix[3 * node + 2]);
+    }
+    free(gfix);
   }
 
   /* 3. grid update (:274-309) */

@@ -30,7 +30,8 @@ class OracleInst(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("domain_h", ctypes.c_double),
                 ("dt", ctypes.c_double), ("actuation", ctypes.c_double),
                 ("contraction", ctypes.c_double), ("freq", ctypes.c_double),
-                ("payload_density", ctypes.c_double), ("axisym", ctypes.c_int32)]
+                ("payload_density", ctypes.c_double), ("axisym", ctypes.c_int32),
+                ("fixed_p2g", ctypes.c_int32)]
 
 
 @dataclass
@@ -45,10 +46,14 @@ class Instance:
     freq: float = 1.0               # mpm_sim.py:149
     payload_density: float = 2.5    # mpm_sim.py:147
     axisym: bool = False            # JELLY_AXISYM, mpm_sim.py:17
+    # not in the reference: P2G sums in 2^-44 fixed point (order-free), as the
+    # GPU engine's deterministic forward sums them; see mpm_oracle.c
+    fixed_p2g: bool = False
 
     def c(self) -> OracleInst:
         return OracleInst(self.nx, self.ny, self.domain_h, self.dt, self.actuation,
-                          self.contraction, self.freq, self.payload_density, 1 if self.axisym else 0)
+                          self.contraction, self.freq, self.payload_density, 1 if self.axisym else 0,
+                          1 if self.fixed_p2g else 0)
 
 
 def build(force: bool = False) -> str:

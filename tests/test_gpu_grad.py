@@ -148,3 +148,83 @@ def test_adjoint_matches_gpu_central_differences():
     for name, h in (("actuation", 10.0), ("contraction", 1e-2), ("freq", 1e-2)):
         fd = (run(dict(prm, **{name: prm[name] + h}))[0] - run(dict(prm, **{name: prm[name] - h}))[0]) / (2 * h)
         assert abs(g[name][0] - fd) <= 0.1 * abs(fd), (name, g[name][0], fd)
+
+
+def _oracle_disp_at(pos, mat, fib, prm, t0, steps, nx=32):
+    from oracle import oracle as O
+    s = O.new_state(pos.astype(np.float64), mat, fib, "f64", nx, nx)
+    inst = O.Instance(nx=nx, ny=nx, domain_h=1.0, **prm)
+    c0 = O.stats_any([s["x"]], [s["material"]])[0, 0]
+    O.run(inst, s, np.float64(t0), steps)
+    return O.stats_any([s["x"]], [s["material"]])[0, 0] - c0
+
+
+def test_waveform_drop_inside_the_rollout_matches_fp64_differences():
+    """The waveform drops from 1 to 0 at phase == contraction
+    (mpm_sim.py:176-180).  With the drop in the middle of a 200-substep
+    rollout (t0 = 0.5 s, freq 1, contraction 0.502: the drop at t = 0.502 s,
+    substep 100), FP64 central differences of the C oracle at h = 1e-3 on the
+    contraction fraction and the frequency multiplier (the drop moves by 25
+    substeps either way) are dominated by the drop: the discrete adjoint alone
+    (and the float64 autograd restatement, which has no drop term) is four
+    orders of magnitude smaller.  The CUDA gradient, with the drop's boundary
+    term, must match the differences within 5 %, and within 2 % their
+    Richardson extrapolation from h = 1e-3 and 5e-4 (the h -> 0 limit)."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    pos, mat, fib, prm = grad_cases.small_tank(seed=7)
+    prm = dict(prm, contraction=0.502, freq=1.0)
+    t0, steps = 0.5, 200
+    e = Engine([InstanceSpec(len(mat), 32, 32, 1.0)], path="plain")
+    e.load(0, pos, mat, fib)
+    e.set_params(**{k: [v] for k, v in prm.items()})
+    e.time = t0
+    e.grad_forward(steps, 50)
+    g = e.grad_backward()
+    assert not e.error_flags().any()
+    e.close()
+
+    def fd(name, h):
+        hi = _oracle_disp_at(pos, mat, fib, dict(prm, **{name: prm[name] + h}), t0, steps)
+        lo = _oracle_disp_at(pos, mat, fib, dict(prm, **{name: prm[name] - h}), t0, steps)
+        return (hi - lo) / (2 * h)
+
+    for name in ("contraction", "freq"):
+        f1, f2 = fd(name, 1e-3), fd(name, 5e-4)
+        limit = f2 + (f2 - f1) / 3.0
+        got = g[name][0]
+        print(f"\n{name}: CUDA {got:.5e}, FP64 differences h=1e-3 {f1:.5e}, h=5e-4 {f2:.5e}, "
+              f"extrapolated {limit:.5e}")
+        assert abs(got - f1) <= 0.05 * abs(f1), (name, got, f1)
+        assert abs(got - limit) <= 0.02 * abs(limit), (name, got, limit)
+    fa = fd("actuation", 1e-2)
+    assert abs(g["actuation"][0] - fa) <= 1e-2 * abs(fa), (g["actuation"][0], fa)
+
+
+def test_gradient_path_reports_nonfinite_states():
+    """A particle with a NaN velocity: the deterministic forward's G2P flags its
+    instance, grad_forward / grad_backward report JF_ERR_NONFINITE (the Python
+    wrapper records it), the other instance stays clean."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    from jellyfih_b200 import _lib as L
+    pos, mat, fib, prm = grad_cases.small_tank(seed=8)
+    e = Engine([InstanceSpec(len(mat), 32, 32, 1.0)] * 2, path="plain")
+    for m in range(2):
+        e.load(m, pos, mat, fib)
+    v = np.zeros((len(mat), 2), np.float32)
+    v[np.flatnonzero(mat == 0)[0]] = np.nan
+    e.write(1, v=v)
+    e.time = 0.0
+    e.grad_forward(10, 5)
+    flags = e.error_flags()
+    assert flags[0] == 0 and flags[1] != 0
+    assert "non-finite" in e.nonfinite_message
+    e.clear_error_flags()
+    e.nonfinite_message = ""
+    for m in range(2):
+        e.load(m, pos, mat, fib)
+    e.write(1, v=v)
+    loss = np.zeros(2)
+    rc = e._lib.jf_grad_forward(e._h, 10, 5, loss.ctypes.data)
+    assert rc == L.JF_ERR_NONFINITE
+    assert np.isfinite(loss[0])
+    e.close()

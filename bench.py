@@ -327,6 +327,58 @@ def grad_leg(inputs, device, stream, steps=2000, checkpoint_every=100):
             "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast}
 
 
+def plain_leg(inputs, spec, device, stream, S, W, K, batched_value, live, points=4, P=50):
+    """The plain per-instance launch path on the batched run's own trajectory.
+
+    The batched value averages substeps W*S .. (W+K)*S of the trajectory from
+    the loaded inputs.  A second batched engine replays that trajectory and
+    stops at the middle of each of `points` equal parts of the window; each
+    state is copied into a plain-path engine, which is timed for P substeps
+    (after 5 untimed ones).  The plain rate is live particles x substeps over
+    the summed time of all points, so batched_over_plain compares the two
+    paths on the same stretch of the trajectory."""
+    import torch
+    from jellyfih_b200 import Engine
+    M = len(inputs)
+    replay = Engine([spec] * M, path="batched", device=device)
+    replay.set_stream(stream)
+    load_all(replay, inputs)
+    replay.time = 0.0
+    targets = [int(W * S + (i + 0.5) * K * S / points) for i in range(points)]
+    done = 0
+    rows = []
+    total_ms = 0.0
+    for target in targets:
+        replay.step(target - done)
+        done = target
+        states = [replay.read(m) for m in range(M)]
+        params, t_now = replay.get_params(), float(replay.time)
+        plain = Engine([spec] * M, path="plain", device=device)
+        plain.set_stream(stream)
+        for m, st in enumerate(states):
+            plain.load(m, st["x"], st["material"], st["fiber"])
+            plain.write(m, v=st["v"], C=st["C"], F=st["F"], Jp=st["Jp"], glow=st["glow"])
+        plain.set_params(**params)
+        plain.time = t_now
+        plain.step(5)
+        plain.sync()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        plain.step(P)
+        p1.record(stream)
+        p1.synchronize()
+        ms = p0.elapsed_time(p1)
+        plain.close()
+        total_ms += ms
+        rows.append({"substep": target, "ms_per_substep": ms / P, "value": live * P / (ms / 1e3)})
+    replay.close()
+    value = live * P * points / (total_ms / 1e3)
+    return {"value": value, "unit": UNIT, "batched_over_plain": batched_value / value,
+            "substeps_per_point": P, "points": rows,
+            "window": f"substeps {W * S}..{(W + K) * S} of the trajectory from the loaded inputs "
+                      "(the batched value's window)"}
+
+
 def tank_leg(engine, M, seed=1000, workers=None):
     """One generation's tanks into the engine: host fill_tank + load (slot
     arrays built on the host and copied) against load_tank (robot on the
@@ -528,9 +580,6 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1)
-    # the state the timed steps ended in, for the plain path's comparison run
-    snapshot = None if (args.no_extras or world > 1) else (
-        [engine.read(m) for m in range(M)], engine.get_params(), float(engine.time))
     kt = engine.kernel_timing()
     engine.set_kernel_timing(False)
     gpu_launches = engine.kernel_launches - launches0
@@ -603,39 +652,9 @@ def run_ours(args):
             extras["e2e"]["gathered_results"] = int(gather_rows(res).shape[0])
 
     if not args.no_extras and world == 1:
-        # plain per-instance launch path (the batched / plain ratio): on the
-        # state the batched timed steps ended in, and from the loaded inputs
-        def time_plain(setup, P=50):
-            plain = Engine([spec] * M, path="plain", device=local)
-            plain.set_stream(stream)
-            setup(plain)
-            plain.step(5)
-            plain.sync()
-            p0 = torch.cuda.Event(enable_timing=True)
-            p1 = torch.cuda.Event(enable_timing=True)
-            p0.record(stream)
-            plain.step(P)
-            p1.record(stream)
-            p1.synchronize()
-            pms = p0.elapsed_time(p1)
-            plain.close()
-            return live * P / (pms / 1e3) * world, pms / P
-
-        def from_snapshot(plain):
-            states, params, t_end = snapshot
-            for m, st in enumerate(states):
-                plain.load(m, st["x"], st["material"], st["fiber"])
-                plain.write(m, v=st["v"], C=st["C"], F=st["F"], Jp=st["Jp"], glow=st["glow"])
-            plain.set_params(**params)
-            plain.time = t_end
-
-        plain_value, plain_ms = time_plain(from_snapshot)
-        load_value, load_ms = time_plain(lambda p: load_all(p, inputs))
-        extras["plain"] = {"value": plain_value, "unit": UNIT, "substeps": 50,
-                           "ms_per_substep": plain_ms, "batched_over_plain": value / plain_value,
-                           "state": "the particle state the batched timed steps ended in",
-                           "from_loaded_inputs": {"value": load_value, "ms_per_substep": load_ms,
-                                                  "batched_over_plain": value / load_value}}
+        # plain per-instance launch path (the batched / plain ratio), timed at
+        # points inside the window of substeps the batched value averages over
+        extras["plain"] = plain_leg(inputs, spec, local, stream, S, W, K, value, live)
 
         extras["differentiable"] = grad_leg(inputs[:8], local, stream, steps=args.grad_substeps)
         if not args.no_refine:

@@ -1,11 +1,15 @@
-"""Autotuner of the batched path: picks cluster size and re-sort interval by
-timing short trials on the caller's own batch.
+"""Autotuner of the batched path: picks the kernel layout (cell tasks, threads
+per CTA, cell cap), the cluster size and the re-sort interval by timing short
+trials on the caller's own batch.
 
-Candidates are the cluster sizes whose shared-memory window fits (CTAs per
-instance: more CTAs give each instance more SMs but more halo rows) and the
-re-sort intervals (longer intervals amortise the counting sort; particles that
-drift out of their cell's register block fall back to per-particle atomics).
-Each trial loads the same particle sets, runs a warm-up chunk, then times
+Candidates are the kernel layouts (split cell tasks at 512, 640 or 768
+threads per CTA, whose launch bounds give 128, 96 or 80 registers per thread;
+lane-per-cell tasks at 512 threads with the cell cap chosen per re-sort or
+fixed), the cluster sizes whose shared-memory window fits (CTAs per instance:
+more CTAs give each instance more SMs but more halo rows) and the re-sort
+intervals (longer intervals amortise the counting sort; particles that drift
+out of their cell's register block fall back to per-particle atomics).  Each
+trial loads the same particle sets, runs a warm-up chunk, then times
 `trial_steps` substeps with CUDA events around every chunk and re-sort launch.
 """
 from __future__ import annotations
@@ -15,22 +19,29 @@ import itertools
 from .engine import Engine
 from ._lib import JfError
 
+# (cell_tasks, block_threads, cell_cap)
+LAYOUTS = (("split", 512, 0), ("split", 640, 0), ("split", 768, 0), ("lane", 512, 0))
+
 
 def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), trial_steps=256,
-             device=0, params=None):
+             device=0, params=None, layouts=LAYOUTS):
     """Returns (best config dict, list of trial results).
 
     `inputs[m]` = (pos, material, fiber); `params` = kwargs of Engine.set_params.
-    Each trial result: dict(cluster_size, resort_interval, ms_per_substep,
-    atomic_scatter_fraction) or an "error" entry for configurations the
-    device cannot run (shared memory, cluster scheduling).
+    The best config holds the Engine keyword arguments cluster_size,
+    resort_interval, cell_tasks, block_threads and cell_cap.  Each trial
+    result: that config plus ms_per_substep and atomic_scatter_fraction, or an
+    "error" entry for configurations the device cannot run (shared memory,
+    cluster scheduling).
     """
     results = []
-    for cs, ri in itertools.product(clusters, resorts):
+    for (tasks, threads, cap), cs, ri in itertools.product(layouts, clusters, resorts):
+        cfg = {"cluster_size": cs, "resort_interval": ri, "cell_tasks": tasks, "block_threads": threads,
+               "cell_cap": cap}
         try:
-            e = Engine(list(specs), path="batched", device=device, resort_interval=ri, cluster_size=cs)
+            e = Engine(list(specs), path="batched", device=device, **cfg)
         except JfError as err:
-            results.append({"cluster_size": cs, "resort_interval": ri, "error": str(err)})
+            results.append(dict(cfg, error=str(err)))
             continue
         try:
             for m, (pos, mat, fib) in enumerate(inputs):
@@ -46,13 +57,15 @@ def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), t
             kt = e.kernel_timing()
             pc = e.path_counts()
             total = pc["register_scatters"] + pc["atomic_scatters"]
-            results.append({"cluster_size": cs, "resort_interval": ri,
-                            "ms_per_substep": (kt["step_ms"] + kt["sort_ms"]) / steps,
-                            "atomic_scatter_fraction": pc["atomic_scatters"] / max(total, 1)})
+            results.append(dict(cfg, ms_per_substep=(kt["step_ms"] + kt["sort_ms"]) / steps,
+                                atomic_scatter_fraction=pc["atomic_scatters"] / max(total, 1)))
+        except JfError as err:
+            results.append(dict(cfg, error=str(err)))
         finally:
             e.close()
     ok = [r for r in results if "ms_per_substep" in r]
     if not ok:
         raise RuntimeError("no batched configuration could run on this device")
     best = min(ok, key=lambda r: r["ms_per_substep"])
-    return {"cluster_size": best["cluster_size"], "resort_interval": best["resort_interval"]}, results
+    return {k: best[k] for k in ("cluster_size", "resort_interval", "cell_tasks", "block_threads",
+                                 "cell_cap")}, results

@@ -63,19 +63,10 @@ typedef struct {
   int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 64 */
   int32_t block_threads;                /* batched: threads per CTA, 0 = 512 */
   int32_t cluster_size;                 /* batched: CTAs per instance (1..16), 0 = automatic */
-  int32_t cell_cap;                     /* batched, JF_CELL_TASKS_LANE: particles a cell lane
-                                           accumulates per substep; the rest of the cell goes
-                                           through per-particle atomics.  0 = chosen per instance at
-                                           every re-sort, >= 16 = no cap.  Not used by split tasks */
-  int32_t cell_tasks;                   /* batched: JF_CELL_TASKS_*, 0 = JF_CELL_TASKS_SPLIT */
+  int32_t cell_cap;                     /* batched: particles a cell lane accumulates per substep;
+                                           the rest of the cell goes through per-particle atomics.
+                                           0 = chosen per instance at every re-sort, >= 16 = no cap */
 } jf_config;
-
-/* How the batched kernel's warps run a 32-cell row segment of their band. */
-#define JF_CELL_TASKS_SPLIT 1  /* the segment's particles one per lane (G2P and material update),
-                                  scatter terms staged in shared memory, then every lane adds its
-                                  own cell's particles to its node block; block_threads <= 768 */
-#define JF_CELL_TASKS_LANE 2   /* one lane per cell runs its cell's particles end to end
-                                  (cell_cap applies); block_threads <= 512 */
 
 /* Engine life cycle.  Replaces the import-time allocation of mpm_sim.py:86-149;
  * per-instance parameters start at the reference defaults (actuation 500,

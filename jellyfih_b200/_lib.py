@@ -25,8 +25,6 @@ JF_VORT_RDBU = 0
 JF_VORT_HUESHIFT = 1
 JF_VORT_WHITE = 2
 JF_NOALLOC_MAX_NODES = 32768
-JF_CELL_TASKS_SPLIT = 1
-JF_CELL_TASKS_LANE = 2
 
 
 class JfInstanceDesc(ctypes.Structure):
@@ -39,7 +37,7 @@ class JfConfig(ctypes.Structure):
                 ("dt", ctypes.c_double), ("path", ctypes.c_int32), ("flags", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("resort_interval", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("cluster_size", ctypes.c_int32),
-                ("cell_cap", ctypes.c_int32), ("cell_tasks", ctypes.c_int32)]
+                ("cell_cap", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p

@@ -1,16 +1,16 @@
-"""Autotuner of the batched path: picks the kernel layout (cell tasks, threads
-per CTA, cell cap), the cluster size and the re-sort interval by timing short
-trials on the caller's own batch.
+"""Autotuner of the batched path: picks the threads per CTA, the cell cap, the
+cluster size and the re-sort interval by timing short trials on the caller's
+own batch.
 
-Candidates are the kernel layouts (split cell tasks at 512, 640 or 768
-threads per CTA, whose launch bounds give 128, 96 or 80 registers per thread;
-lane-per-cell tasks at 512 threads with the cell cap chosen per re-sort or
-fixed), the cluster sizes whose shared-memory window fits (CTAs per instance:
-more CTAs give each instance more SMs but more halo rows) and the re-sort
-intervals (longer intervals amortise the counting sort; particles that drift
-out of their cell's register block fall back to per-particle atomics).  Each
-trial loads the same particle sets, runs a warm-up chunk, then times
-`trial_steps` substeps with CUDA events around every chunk and re-sort launch.
+Candidates are the kernel layouts (threads per CTA: fewer warps per SM leave
+more registers and L1 per warp but hide less latency; the cell cap chosen by
+the sort's cost model at every re-sort, or fixed), the cluster sizes whose
+shared-memory window fits (CTAs per instance: more CTAs give each instance
+more SMs but more halo rows) and the re-sort intervals (longer intervals
+amortise the counting sort; particles that drift out of their cell's register
+block fall back to per-particle atomics).  Each trial loads the same particle
+sets, runs a warm-up chunk, then times `trial_steps` substeps with CUDA events
+around every chunk and re-sort launch.
 """
 from __future__ import annotations
 
@@ -19,8 +19,8 @@ import itertools
 from .engine import Engine
 from ._lib import JfError
 
-# (cell_tasks, block_threads, cell_cap)
-LAYOUTS = (("split", 512, 0), ("split", 640, 0), ("split", 768, 0), ("lane", 512, 0))
+# (block_threads, cell_cap); cell_cap 0 = chosen by the cost model at every re-sort
+LAYOUTS = ((512, 0), (384, 0), (512, 4))
 
 
 def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), trial_steps=256,
@@ -29,15 +29,14 @@ def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), t
 
     `inputs[m]` = (pos, material, fiber); `params` = kwargs of Engine.set_params.
     The best config holds the Engine keyword arguments cluster_size,
-    resort_interval, cell_tasks, block_threads and cell_cap.  Each trial
+    resort_interval, block_threads and cell_cap.  Each trial
     result: that config plus ms_per_substep and atomic_scatter_fraction, or an
     "error" entry for configurations the device cannot run (shared memory,
     cluster scheduling).
     """
     results = []
-    for (tasks, threads, cap), cs, ri in itertools.product(layouts, clusters, resorts):
-        cfg = {"cluster_size": cs, "resort_interval": ri, "cell_tasks": tasks, "block_threads": threads,
-               "cell_cap": cap}
+    for (threads, cap), cs, ri in itertools.product(layouts, clusters, resorts):
+        cfg = {"cluster_size": cs, "resort_interval": ri, "block_threads": threads, "cell_cap": cap}
         try:
             e = Engine(list(specs), path="batched", device=device, **cfg)
         except JfError as err:
@@ -67,5 +66,4 @@ def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), t
     if not ok:
         raise RuntimeError("no batched configuration could run on this device")
     best = min(ok, key=lambda r: r["ms_per_substep"])
-    return {k: best[k] for k in ("cluster_size", "resort_interval", "cell_tasks", "block_threads",
-                                 "cell_cap")}, results
+    return {k: best[k] for k in ("cluster_size", "resort_interval", "block_threads", "cell_cap")}, results

@@ -54,24 +54,6 @@ constexpr int kRowCost = 40;  // grid update of one row, in the cost model's uni
 constexpr int kSolidCostHalves = 3;
 constexpr int kNoCap = 1 << 30;
 
-// Split cell tasks (JF_CELL_TASKS_SPLIT): a warp first runs the particles of
-// its 32-cell row segment one per lane (G2P, then P2G's material update), and
-// stages each particle's scatter terms in shared memory; then each lane
-// accumulates the staged particles of its own cell into its 4x4 node block
-// and the warp flushes the blocks.  The accumulator is live only in the
-// second phase, so the first phase (the SVD and stress chain) and the second
-// never hold their registers at once, and the first phase keeps every lane
-// busy whatever the cells' counts.  A segment is staged kStage particles at a
-// time; a staged particle is 9 floats (position, APIC affine, momentum, mass),
-// kept as planes with one pad word per 32 entries so that lanes reading
-// entries four apart (four particles per cell) hit distinct banks.
-constexpr int kStageLane = 4;
-constexpr int kStage = 32 * kStageLane;
-constexpr int kStagePitch = kStage + kStage / 32;
-constexpr int kStagePlanes = 9;
-constexpr int kStageWarpFloats = kStagePlanes * kStagePitch;
-__device__ __forceinline__ int stage_pos(int i) { return i + (i >> 5); }
-
 // Sort cell of a particle: (floor(X - 1/4), floor(Y - 1/4)) in grid units,
 // clamped at 0.  The stencil base trunc(X - 1/2) of a particle in sort cell k
 // is k - 1 or k, so a lane that owns cell k accumulates a 4x4 node block.
@@ -107,7 +89,6 @@ struct ChunkArgs {
   int32_t* err;
   int32_t M;
   int32_t CS;
-  int32_t win_planes;       // planes of the shared-memory window (5, 6 axisymmetric)
   int32_t K;                // substeps in this chunk
   const float* t_dev;       // sim_time at the chunk's start (device scalar)
   float dt;
@@ -169,11 +150,9 @@ __device__ __forceinline__ float2 gather_node(const Window& w, cg::cluster_group
 }
 
 // Scatter of one particle's 9 stencil contributions with atomics, local when
-// the rows are in this CTA's window, else into the owner CTA's window (the
-// axisymmetric hoop channel too unless with_hoop is false).
+// the rows are in this CTA's window, else into the owner CTA's window.
 __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_group& cl, const JfInst& I,
-                                                 const JfStencil& st, const JfScatter& sc,
-                                                 bool with_hoop = true) {
+                                                 const JfStencil& st, const JfScatter& sc) {
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int row = st.by + j;
@@ -186,7 +165,7 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
         atomicAdd(w.Ax + rn + i, c.x);
         atomicAdd(w.Ay + rn + i, c.y);
         atomicAdd(w.Am + rn + i, c.z);
-        if (I.axisym && with_hoop) atomicAdd(w.Ah + rn + i, jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
+        if (I.axisym) atomicAdd(w.Ah + rn + i, jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
       }
     } else {
       const int o = owner_of(w, row);
@@ -197,30 +176,8 @@ __device__ __forceinline__ void scatter_particle(const Window& w, cg::cluster_gr
         dsmem_add(dsmem_addr(w.Ax + rn + i, o), c.x);
         dsmem_add(dsmem_addr(w.Ay + rn + i, o), c.y);
         dsmem_add(dsmem_addr(w.Am + rn + i, o), c.z);
-        if (I.axisym && with_hoop)
-          dsmem_add(dsmem_addr(w.Ah + rn + i, o), jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
+        if (I.axisym) dsmem_add(dsmem_addr(w.Ah + rn + i, o), jf_w(st, 0, i) * jf_w(st, 1, j) * sc.hoop);
       }
-    }
-  }
-}
-
-// The axisymmetric hoop channel of one particle alone (split cell tasks add
-// it when the particle's material update runs, before its other channels are
-// staged), local or in the row owner's window.
-__device__ __forceinline__ void scatter_hoop(const Window& w, const JfStencil& st, float hoop) {
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const int row = st.by + j;
-    const int wr = row - w.win0;
-    if (wr >= 0 && wr < w.VR) {
-      const int rn = wr * w.nx + st.bx;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) atomicAdd(w.Ah + rn + i, jf_w(st, 0, i) * jf_w(st, 1, j) * hoop);
-    } else {
-      const int o = owner_of(w, row);
-      const int rn = owner_row(w, row, o) * w.nx + st.bx;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) dsmem_add(dsmem_addr(w.Ah + rn + i, o), jf_w(st, 0, i) * jf_w(st, 1, j) * hoop);
     }
   }
 }
@@ -300,8 +257,7 @@ __device__ __forceinline__ void flush_block(const float* acc, const Window& w, i
   }
 }
 
-template <int kSplit, int kThreads>
-__global__ void __launch_bounds__(kThreads, 1) chunk_kernel(ChunkArgs a) {
+__global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
   // per-substep values, double-buffered so that substep s + 1's are set
@@ -339,8 +295,6 @@ __global__ void __launch_bounds__(kThreads, 1) chunk_kernel(ChunkArgs a) {
   w.Am = w.Ay + WN;
   w.Ah = w.Am + WN;  // a sixth plane exists only in the axisymmetric variant
   const int n_planes = I.axisym ? 6 : 5;
-  // split cell tasks: this warp's staging area after the window's planes
-  float* const stg = sm + (size_t)a.win_planes * WN + (size_t)(threadIdx.x >> 5) * kStageWarpFloats;
   const int cap = a.cap[m];
   const int tid = threadIdx.x, nth = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, n_warps = nth >> 5;
@@ -447,204 +401,98 @@ __global__ void __launch_bounds__(kThreads, 1) chunk_kernel(ChunkArgs a) {
       const int cy = row0 + task / segs;
       const int seg0 = (task % segs) << 5;
       const int cx = seg0 + lane;
-      if constexpr (kSplit == 0) {
-        int beg = 0, end = 0;
-        if (cx < nx) {
-          const int c = cy * nx + cx;
-          beg = cstart[c];
-          end = min(cstart[c + 1], beg + cap);  // the rest of the cell is overflow
-        }
-        // 4x4 node block: columns cx-1 .. cx+2, rows cy-1 .. cy+2
-        float acc[48];
+      int beg = 0, end = 0;
+      if (cx < nx) {
+        const int c = cy * nx + cx;
+        beg = cstart[c];
+        end = min(cstart[c + 1], beg + cap);  // the rest of the cell is overflow
+      }
+      // 4x4 node block: columns cx-1 .. cx+2, rows cy-1 .. cy+2
+      float acc[48];
 #pragma unroll
-        for (int q = 0; q < 48; ++q) acc[q] = 0.0f;
-        float4 nxv;
-        int nmt = -1;
-        if (beg < end) {
-          nxv = xv_m[beg];
-          nmt = mat_m[beg];
+      for (int q = 0; q < 48; ++q) acc[q] = 0.0f;
+      float4 nxv;
+      int nmt = -1;
+      if (beg < end) {
+        nxv = xv_m[beg];
+        nmt = mat_m[beg];
+      }
+      for (int k = beg; k < end; ++k) {
+        const float4 xv = nxv;
+        const int mt = nmt;
+        float4 F = F_m[k];  // first used by P2G, after the gather
+        if (k + 1 < end) {  // next particle of this cell, loaded while this one computes
+          nxv = xv_m[k + 1];
+          nmt = mat_m[k + 1];
         }
-        for (int k = beg; k < end; ++k) {
-          const float4 xv = nxv;
-          const int mt = nmt;
-          float4 F = F_m[k];  // first used by P2G, after the gather
-          if (k + 1 < end) {  // next particle of this cell, loaded while this one computes
-            nxv = xv_m[k + 1];
-            nmt = mat_m[k + 1];
-          }
-          float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
-          float jp = 1.0f;
-          if (mt == 2 || a.do_glow) jp = a.Jp[p0 + k];
-          // G2P replaces v and C from the grid (mpm_sim.py:315-327); the stored
-          // C is read only where G2P does not run
-          float4 C;
-          if (do_g2p) {
-            JfStencil st;
-            if (!jf_stencil(I, x, st)) {
-              C = C_m[k];
-            } else {
-              const int wr0 = st.by - w.win0;
-              if (wr0 >= 0 && wr0 + 2 < w.VR) {
-                const int wb = wr0 * nx + st.bx;
-                jf_g2p_apic(I, st, v, C, [&](int i, int j) {
-                  const int n = wb + j * nx + i;
-                  return w.G[n];
-                });
-              } else {
-                ++n_gather_generic;
-                jf_g2p_apic(I, st, v, C,
-                            [&](int i, int j) { return gather_node(w, cluster, st.bx + i, st.by + j); });
-              }
-            }
-            jf_g2p_advect(I, x, v);
-            if (a.do_glow) a.glow[p0 + k] = jf_glow(a.glow[p0 + k], jp);
-            if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
-            xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
-            // this pass's P2G takes C from registers and the next pass's G2P
-            // recomputes it, so C is stored only by the chunk's last pass and
-            // where the particle leaves the stencil range (P2G below)
-            if (!do_p2g) C_m[k] = C;
-          } else {
+        float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+        float jp = 1.0f;
+        if (mt == 2 || a.do_glow) jp = a.Jp[p0 + k];
+        // G2P replaces v and C from the grid (mpm_sim.py:315-327); the stored
+        // C is read only where G2P does not run
+        float4 C;
+        if (do_g2p) {
+          JfStencil st;
+          if (!jf_stencil(I, x, st)) {
             C = C_m[k];
-          }
-          if (do_p2g) {
-            JfStencil st;
-            if (jf_stencil(I, x, st)) {
-              const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
-              JfScatter sc;
-              jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
-                              I.axisym ? a.rref[p0 + k] : 1.0f);
-              F_m[k] = F;
-              if (mt == 2) a.Jp[p0 + k] = jp;
-              const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
-              const bool in_block = (unsigned)di < 2u && (unsigned)dj < 2u;
-              n_fast += in_block ? 1u : 0u;
-              n_generic += in_block ? 0u : 1u;
-              if (in_block) {
-                accumulate_block(acc, I, st, sc, di, dj);
-                if (I.axisym) {  // the hoop sum goes straight to the window (rows in it)
-                  const int hb = (st.by - w.win0) * nx + st.bx;
-#pragma unroll
-                  for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                    for (int ii = 0; ii < 3; ++ii)
-                      atomicAdd(w.Ah + hb + jj * nx + ii, jf_w(st, 0, ii) * jf_w(st, 1, jj) * sc.hoop);
-                }
-              } else {
-                scatter_particle(w, cluster, I, st, sc);
-              }
-            } else if (do_g2p) {
-              C_m[k] = C;  // out of range: the next G2P keeps this C
-            }
-          }
-        }
-        __syncwarp();
-        if (do_p2g) flush_block(acc, w, lane, cx, cy, seg0, nx);
-      } else {
-        // split cell task: the segment's particles one per lane, in rounds of
-        // kStage (phase A), then each lane's own cell from the staging (phase B)
-        const unsigned full = 0xffffffffu;
-        const int c = cy * nx + min(cx, nx);  // lanes past the row's end: an empty run at its end
-        const int cs = cstart[c];
-        const int ce = (cx < nx) ? cstart[c + 1] : cs;
-        const int seg_beg = __shfl_sync(full, cs, 0);
-        const int seg_end = __shfl_sync(full, ce, min(31, nx - 1 - seg0));
-        for (int rb = seg_beg; rb < seg_end; rb += kStage) {
-          const int nr = min(kStage, seg_end - rb);
-          for (int i = lane; i < nr; i += 32) {
-            const int k = rb + i;
-            const float4 xv = xv_m[k];
-            const int mt = mat_m[k];
-            float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
-            float jp = 1.0f;
-            if (mt == 2 || a.do_glow) jp = a.Jp[p0 + k];
-            float4 C;
-            if (do_g2p) {
-              JfStencil st;
-              if (!jf_stencil(I, x, st)) {
-                C = C_m[k];
-              } else {
-                const int wr0 = st.by - w.win0;
-                if (wr0 >= 0 && wr0 + 2 < w.VR) {
-                  const int wb = wr0 * nx + st.bx;
-                  jf_g2p_apic(I, st, v, C, [&](int ii, int jj) { return w.G[wb + jj * nx + ii]; });
-                } else {
-                  ++n_gather_generic;
-                  jf_g2p_apic(I, st, v, C,
-                              [&](int ii, int jj) { return gather_node(w, cluster, st.bx + ii, st.by + jj); });
-                }
-              }
-              jf_g2p_advect(I, x, v);
-              if (a.do_glow) a.glow[p0 + k] = jf_glow(a.glow[p0 + k], jp);
-              if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
-              xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
-              if (!do_p2g) C_m[k] = C;
+          } else {
+            const int wr0 = st.by - w.win0;
+            if (wr0 >= 0 && wr0 + 2 < w.VR) {
+              const int wb = wr0 * nx + st.bx;
+              jf_g2p_apic(I, st, v, C, [&](int i, int j) {
+                const int n = wb + j * nx + i;
+                return w.G[n];
+              });
             } else {
-              C = C_m[k];
-            }
-            if (do_p2g) {
-              const int q = stage_pos(i);
-              JfStencil st;
-              if (jf_stencil(I, x, st)) {
-                float4 F = F_m[k];
-                const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
-                JfScatter sc;
-                jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
-                                I.axisym ? a.rref[p0 + k] : 1.0f);
-                F_m[k] = F;
-                if (mt == 2) a.Jp[p0 + k] = jp;
-                if (I.axisym) scatter_hoop(w, st, sc.hoop);
-                stg[0 * kStagePitch + q] = x.x;
-                stg[1 * kStagePitch + q] = x.y;
-                stg[2 * kStagePitch + q] = sc.af00;
-                stg[3 * kStagePitch + q] = sc.af01;
-                stg[4 * kStagePitch + q] = sc.af10;
-                stg[5 * kStagePitch + q] = sc.af11;
-                stg[6 * kStagePitch + q] = sc.mv0;
-                stg[7 * kStagePitch + q] = sc.mv1;
-                stg[8 * kStagePitch + q] = sc.mass;
-              } else {
-                if (do_g2p) C_m[k] = C;  // out of range: the next G2P keeps this C
-                stg[0 * kStagePitch + q] = -1.0f;  // no scatter (outside every stencil range)
-              }
+              ++n_gather_generic;
+              jf_g2p_apic(I, st, v, C,
+                          [&](int i, int j) { return gather_node(w, cluster, st.bx + i, st.by + j); });
             }
           }
-          __syncwarp();
-          if (do_p2g) {
-            float acc[48];
+          jf_g2p_advect(I, x, v);
+          if (a.do_glow) a.glow[p0 + k] = jf_glow(a.glow[p0 + k], jp);
+          if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
+          xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
+          // this pass's P2G takes C from registers and the next pass's G2P
+          // recomputes it, so C is stored only by the chunk's last pass and
+          // where the particle leaves the stencil range (P2G below)
+          if (!do_p2g) C_m[k] = C;
+        } else {
+          C = C_m[k];
+        }
+        if (do_p2g) {
+          JfStencil st;
+          if (jf_stencil(I, x, st)) {
+            const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
+            JfScatter sc;
+            jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
+                            I.axisym ? a.rref[p0 + k] : 1.0f);
+            F_m[k] = F;
+            if (mt == 2) a.Jp[p0 + k] = jp;
+            const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
+            const bool in_block = (unsigned)di < 2u && (unsigned)dj < 2u;
+            n_fast += in_block ? 1u : 0u;
+            n_generic += in_block ? 0u : 1u;
+            if (in_block) {
+              accumulate_block(acc, I, st, sc, di, dj);
+              if (I.axisym) {  // the hoop sum goes straight to the window (rows in it)
+                const int hb = (st.by - w.win0) * nx + st.bx;
 #pragma unroll
-            for (int qq = 0; qq < 48; ++qq) acc[qq] = 0.0f;
-            const int lo = max(cs, rb) - rb, hi = min(ce, rb + nr) - rb;
-            for (int i = lo; i < hi; ++i) {
-              const int q = stage_pos(i);
-              const float2 x = make_float2(stg[0 * kStagePitch + q], stg[1 * kStagePitch + q]);
-              JfStencil st;
-              if (!jf_stencil(I, x, st)) continue;
-              JfScatter sc;
-              sc.af00 = stg[2 * kStagePitch + q];
-              sc.af01 = stg[3 * kStagePitch + q];
-              sc.af10 = stg[4 * kStagePitch + q];
-              sc.af11 = stg[5 * kStagePitch + q];
-              sc.mv0 = stg[6 * kStagePitch + q];
-              sc.mv1 = stg[7 * kStagePitch + q];
-              sc.mass = stg[8 * kStagePitch + q];
-              sc.hoop = 0.0f;
-              const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
-              const bool in_block = (unsigned)di < 2u && (unsigned)dj < 2u;
-              n_fast += in_block ? 1u : 0u;
-              n_generic += in_block ? 0u : 1u;
-              if (in_block) {
-                accumulate_block(acc, I, st, sc, di, dj);
-              } else {
-                scatter_particle(w, cluster, I, st, sc, false);
+                for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                  for (int ii = 0; ii < 3; ++ii)
+                    atomicAdd(w.Ah + hb + jj * nx + ii, jf_w(st, 0, ii) * jf_w(st, 1, jj) * sc.hoop);
               }
+            } else {
+              scatter_particle(w, cluster, I, st, sc);
             }
-            __syncwarp();
-            flush_block(acc, w, lane, cx, cy, seg0, nx);
+          } else if (do_g2p) {
+            C_m[k] = C;  // out of range: the next G2P keeps this C
           }
-          __syncwarp();
         }
       }
+      __syncwarp();
+      if (do_p2g) flush_block(acc, w, lane, cx, cy, seg0, nx);
       int nt = 0;
       if (lane == 0) nt = atomicAdd(next_task, 1);
       task_id = __shfl_sync(0xffffffffu, nt, 0);
@@ -790,8 +638,7 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
                                                                 int32_t* __restrict__ cap_out,
                                                                 int32_t* __restrict__ ovband,
                                                                 int32_t* __restrict__ ovcur, int CS,
-                                                                int fixed_cap, const int32_t* __restrict__ solid,
-                                                                int split) {
+                                                                int fixed_cap, const int32_t* __restrict__ solid) {
   __shared__ int warp_sums[kScanThreads / 32];
   __shared__ int s_cost[kCapCandidates];
   __shared__ int s_row_cost[kMaxBandRows];
@@ -847,18 +694,13 @@ __global__ void __launch_bounds__(kScanThreads) sort_scan_kernel(const JfInst* _
     const int x0 = (sg - row * segs) << 5;
     const int xn = min(32, I.nx - x0);
     const int32_t* cr = c + row * I.nx + x0;
-    int mx = 0, ov = 0, sum = 0;
+    int mx = 0, ov = 0;
     for (int i = 0; i < xn; ++i) {
       mx = max(mx, cr[i]);
       ov += max(0, cr[i] - cap);
-      sum += cr[i];
     }
     if (dynamic) {
-      // split tasks: the segment's particles one per lane (4 per particle),
-      // then the lanes' own cells, about a sixth of a particle's work each
-      // (24 per particle of the fullest cell); lane tasks: the fullest cell's
-      // capped count for the whole warp plus the overflow
-      atomicAdd(&s_row_cost[row], split ? 4 * sum + 24 * mx : 128 * min(mx, cap) + 6 * ov);
+      atomicAdd(&s_row_cost[row], 128 * min(mx, cap) + 6 * ov);
       if (ov) atomicAdd(&s_row_over[row], ov);
     } else if (ov) {
       atomicAdd(&s_row_over[min(row / I.band_h, CS - 1)], ov);  // per band
@@ -1007,23 +849,8 @@ __global__ void advance_time_kernel(float* t, int K, float dt) {
 
 size_t jf_batched_smem_bytes(const jf_engine* e) {
   const size_t planes = (e->flags & JF_FLAG_AXISYM) ? 6 : 5;
-  size_t bytes = sizeof(float) * planes * (size_t)e->win_nodes;
-  if (e->cell_tasks == JF_CELL_TASKS_SPLIT) bytes += sizeof(float) * kStageWarpFloats * (size_t)(e->block_threads / 32);
-  return bytes;
+  return sizeof(float) * planes * (size_t)e->win_nodes;
 }
-
-namespace {
-using ChunkFn = void (*)(ChunkArgs);
-
-// The chunk kernel instance for the engine's cell tasks and block size
-// (each instance's launch bound sets its register budget).
-ChunkFn chunk_fn(const jf_engine* e) {
-  if (e->cell_tasks == JF_CELL_TASKS_LANE) return chunk_kernel<0, 512>;
-  if (e->block_threads <= 512) return chunk_kernel<1, 512>;
-  if (e->block_threads <= 640) return chunk_kernel<1, 640>;
-  return chunk_kernel<1, 768>;
-}
-}  // namespace
 
 cudaError_t jf_batched_sort(jf_engine* e) {
   JfTimed timed(e, true, e->capturing);
@@ -1039,10 +866,7 @@ cudaError_t jf_batched_sort(jf_engine* e) {
   }
   sort_scan_kernel<<<e->M, kScanThreads, 0, e->stream>>>(e->d_inst, e->d_counts, stride, e->d_band,
                                                          e->d_brow, e->d_cap, e->d_ovband, e->d_ovcur,
-                                                         e->cluster,
-                                                         e->cell_tasks == JF_CELL_TASKS_SPLIT ? kCapCandidates
-                                                                                              : e->cell_cap,
-                                                         e->d_solid, e->cell_tasks == JF_CELL_TASKS_SPLIT ? 1 : 0);
+                                                         e->cluster, e->cell_cap, e->d_solid);
   if (e->max_slots > 0) {
     sort_scatter_kernel<<<grid, kSortThreads, 0, e->stream>>>(e->d_inst, e->d_keys, e->d_rank, e->d_counts,
                                                              stride, e->d_cap, e->cluster, e->d_brow,
@@ -1080,7 +904,6 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   a.err = e->d_err;
   a.M = e->M;
   a.CS = e->cluster;
-  a.win_planes = (e->flags & JF_FLAG_AXISYM) ? 6 : 5;
   a.K = K;
   a.t_dev = e->d_time;
   a.dt = (float)e->dt;
@@ -1102,7 +925,7 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   cudaError_t err;
   {
     JfTimed timed(e, false, e->capturing);
-    err = cudaLaunchKernelEx(&cfg, chunk_fn(e), a);
+    err = cudaLaunchKernelEx(&cfg, chunk_kernel, a);
   }
   e->launches += 1;
   if (err != cudaSuccess) return err;
@@ -1116,11 +939,11 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
 
 cudaError_t jf_batched_prepare(jf_engine* e) {
   const size_t smem = jf_batched_smem_bytes(e);
-  const ChunkFn fn = chunk_fn(e);
-  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = cudaFuncSetAttribute(chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
   if (err != cudaSuccess) return err;
   if (e->cluster > 8) {
-    err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    err = cudaFuncSetAttribute(chunk_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (err != cudaSuccess) return err;
   }
   return cudaSuccess;
@@ -1138,7 +961,7 @@ int jf_batched_max_active_clusters(jf_engine* e, int cluster, int* out) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return (int)cudaOccupancyMaxActiveClusters(out, chunk_fn(e), &cfg);
+  return (int)cudaOccupancyMaxActiveClusters(out, chunk_kernel, &cfg);
 }
 
 static cudaError_t chunk_with_sort(jf_engine* e, int K) {

@@ -257,7 +257,6 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 64;
   e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
   e->cell_cap = cfg->cell_cap;
-  e->cell_tasks = cfg->cell_tasks > 0 ? cfg->cell_tasks : JF_CELL_TASKS_SPLIT;
   e->use_graphs = (cfg->flags & JF_FLAG_NO_GRAPHS) == 0;
   auto bail = [&](int code, const std::string& msg) {
     jf_set_global_error(msg);
@@ -265,16 +264,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     return code;
   };
   if (cfg->cell_cap < 0) return bail(JF_ERR_INVALID, "cell_cap must be >= 0");
-  if (e->cell_tasks != JF_CELL_TASKS_SPLIT && e->cell_tasks != JF_CELL_TASKS_LANE)
-    return bail(JF_ERR_INVALID, "unknown cell_tasks");
-  if (e->cell_tasks == JF_CELL_TASKS_SPLIT && cfg->cell_cap > 0)
-    return bail(JF_ERR_INVALID, "cell_cap applies to JF_CELL_TASKS_LANE only");
-  {
-    const int max_threads = e->cell_tasks == JF_CELL_TASKS_SPLIT ? 768 : 512;
-    if (e->block_threads > max_threads || e->block_threads % 32)
-      return bail(JF_ERR_INVALID, "block_threads must be a multiple of 32, <= " + std::to_string(max_threads) +
-                                      " for these cell tasks");
-  }
+  if (e->block_threads > 512 || e->block_threads % 32) return bail(JF_ERR_INVALID, "block_threads must be a multiple of 32, <= 512");
 
   int ny_max = 0;
   for (int m = 0; m < e->M; ++m) {

@@ -42,7 +42,6 @@ struct jf_engine {
   int32_t resort_interval = 16;
   int32_t block_threads = 512;
   int32_t cluster = 4;
-  int32_t cell_tasks = JF_CELL_TASKS_SPLIT;  // batched: how a warp runs a row segment (JF_CELL_TASKS_*)
 
   std::vector<JfInst> inst;        // host copy
   std::vector<JfParams> params;    // host mirror (authoritative)

@@ -45,16 +45,12 @@ class Engine:
     instance and substep, as the reference's substep() offloads do.
     ``axisym=True`` runs the axisymmetric (r, z) substep of JELLY_AXISYM=1
     (every instance; the load positions' x becomes each particle's r_ref).
-    ``cell_tasks`` picks how the batched kernel's warps run a 32-cell row
-    segment: ``'split'`` (the segment's particles one per lane, then each lane
-    accumulates its own cell's; up to 768 threads per CTA) or ``'lane'`` (a
-    lane per cell end to end, with ``cell_cap``; up to 512 threads).
     """
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
                  block_threads: int = 512, cluster_size: int = 0, graphs: bool = True,
-                 cell_cap: int = 0, axisym: bool = False, cell_tasks: str = "split"):
+                 cell_cap: int = 0, axisym: bool = False):
         self._lib = L.load()
         self.instances = list(instances)
         self.M = len(self.instances)
@@ -63,9 +59,8 @@ class Engine:
             L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
         flags = ((L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
                  | (L.JF_FLAG_AXISYM if axisym else 0))
-        tasks = {"split": L.JF_CELL_TASKS_SPLIT, "lane": L.JF_CELL_TASKS_LANE}[cell_tasks]
         cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
-                         flags, device, resort_interval, block_threads, cluster_size, cell_cap, tasks)
+                         flags, device, resort_interval, block_threads, cluster_size, cell_cap)
         h = L._E()
         rc = self._lib.jf_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != L.JF_OK:
@@ -74,8 +69,7 @@ class Engine:
         self.dt = dt
         self.nonfinite_message = ""  # set when a run reported a non-finite particle state
         self.config = dict(path=path, resort_interval=resort_interval, block_threads=block_threads,
-                           cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap, axisym=axisym,
-                           cell_tasks=cell_tasks)
+                           cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap, axisym=axisym)
 
     # -- plumbing --------------------------------------------------------
     def _check(self, rc):

@@ -247,6 +247,7 @@ struct AdjArgs {
   float2* vtmp;        // velocity adjoint of particles outside the stencil range
   double* gparam;      // M x 3: d/d actuation, d/d contraction, d/d freq
   double* dLdp;        // M: d L / d pressure of this substep, per instance
+  double* fac;         // M x 3: d pressure / d (actuation, contraction, freq) of this substep
 };
 
 __device__ __forceinline__ float wd(int k, float f) {  // d W_k / d f
@@ -317,9 +318,29 @@ __global__ void ad_g2p(AdjArgs A) {
   A.vtmp[g] = make_float2(0.0f, 0.0f);
 }
 
+// d pressure / d (actuation, contraction, freq) of instance m at time t: the
+// activation a, A da/dc and A da/df (mpm_sim.py:173-180; the drop at
+// phase == c is added on the host, see add_waveform_drop_terms).
+__device__ __forceinline__ void pressure_factors(const JfParams& P, float tf, double* fac) {
+  const double f = P.freq, c = P.contraction, t = tf;
+  const float act = jf_activation(P.freq, P.contraction, tf);
+  const double period = 1.0 / f;
+  const double phase = (t - period * floor(t / period)) / period;
+  double da_dc = 0.0, da_df = 0.0;
+  if (act != 0.0f && phase < c) {
+    const double sn = 0.5 * sin(3.14159265 * phase / c);
+    da_dc = sn * 3.14159265 * (-phase / (c * c));
+    da_df = sn * (3.14159265 / c) * t;
+  }
+  fac[0] = act;
+  fac[1] = P.actuation * da_dc;
+  fac[2] = P.actuation * da_df;
+}
+
 __global__ void ad_grid(AdjArgs A) {
   const GradArgs& a = A.f;
   const int m = blockIdx.y;
+  if (blockIdx.x == 0 && threadIdx.x == 0) pressure_factors(a.params[m], a.t, A.fac + 3 * m);
   const JfInst I = a.inst[m];
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= I.nx * I.ny) return;
@@ -345,164 +366,186 @@ __global__ void ad_grid(AdjArgs A) {
   A.pmbar[node] = make_float4(a0, a1, -(a0 * px + a1 * py) / pm, 0.0f);
 }
 
-__global__ void ad_p2g(AdjArgs A) {
+// The P2G adjoint of one live particle g of instance m.  kWater: only water
+// particles whose singular values are both above the 1e-6 floor are done here
+// (closed-form Jacobian: J = det F*, dJ = cof F*, F_out = sqrt(J) I,
+// tau = lambda J (J - 1) I; mpm_sim.py:219-227 with mu = 0), and false is
+// returned for every other particle in range (it goes to the second kernel);
+// otherwise the material map is differentiated with dual numbers.  Returns
+// true when the particle is done; *pbar = d L / d pressure of the particle.
+template <bool kWater>
+__device__ __forceinline__ bool ad_p2g_particle(const AdjArgs& A, const JfInst& I, int m, int64_t g, int mt,
+                                                float pressure, float* pbar) {
+  const GradArgs& a = A.f;
+  *pbar = 0.0f;
+  const float4 xv = a.s.xv[g];
+  const float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
+  JfStencil st;
+  const float2 xt = A.xtmp[g];
+  if (!jf_stencil_strict(I, x, st)) {
+    A.lxv[g] = make_float4(xt.x, xt.y, A.vtmp[g].x, A.vtmp[g].y);
+    return true;  // C and F pass through unchanged outside the stencil range
+  }
+  if (kWater && mt != 0) return false;
+  const float4 C = a.s.C[g], F = a.s.F[g];
+  const float dt = I.dt;
+  const float M00 = radd(1.0f, rmul(dt, C.x)), M01 = rmul(dt, C.y);
+  const float M10 = rmul(dt, C.z), M11 = radd(1.0f, rmul(dt, C.w));
+  const float fsv[4] = {rdot2(M00, F.x, M01, F.z), rdot2(M00, F.y, M01, F.w),
+                        rdot2(M10, F.x, M11, F.z), rdot2(M10, F.y, M11, F.w)};
+  const int ms = jf_mat_slot(mt);
+  const JfMaterials& mats = a.mats;
+  const float la = ms == 0 ? mats.la[0] : ms == 1 ? mats.la[1] : ms == 2 ? mats.la[2]
+                 : ms == 3 ? mats.la[3] : mats.la[4];
+  const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
+  // the material map F* -> (F_out, tau): values and Jacobians d./dF*[e]
+  float tv[4];        // tau values
+  D4 Fo[4], tau[4], J;  // full path: values and Jacobians
+  float dJ[4], kf = 0.0f, kt = 0.0f;  // water path: J = det F*, dJ = cof F*
+  if constexpr (kWater) {
+    // water, no singular value at the 1e-6 floor: J = s1 s2 = det F*, so
+    // dJ = cof F*, dF_out = dJ / (2 sqrt J) I, dtau = lambda (2 J - 1) dJ I;
+    // values as the forward rounds them
+    const JfSvdRot rot = jf_svd2_values(make_float4(fsv[0], fsv[1], fsv[2], fsv[3]));
+    if (!(rot.s1 > 1e-6f && rot.s2 > 1e-6f)) return false;
+    const float Jw = rmul(rot.s1, rot.s2);
+    dJ[0] = fsv[3]; dJ[1] = -fsv[2]; dJ[2] = -fsv[1]; dJ[3] = fsv[0];
+    kf = 0.5f / sqrtf(Jw);
+    kt = la * (2.0f * Jw - 1.0f);
+    const float diag = rmul(rmul(la, Jw), rsub(Jw, 1.0f));
+    tv[0] = diag; tv[1] = 0.0f; tv[2] = 0.0f; tv[3] = diag;
+  } else {
+    const float mu = ms == 0 ? mats.mu[0] : ms == 1 ? mats.mu[1] : ms == 2 ? mats.mu[2]
+                   : ms == 3 ? mats.mu[3] : mats.mu[4];
+    D4 Fs[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      Fs[q] = d4c(fsv[q]);
+      Fs[q].d[q] = 1.0f;
+    }
+    jf_phi<D4>(Fs, mt, mu, la, pressure, fb, Fo, tau, J);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) tv[q] = tau[q].v;
+  }
+  float mass = I.p_mass;
+  if (mt == 2) mass = mass * a.params[m].payload_density;
+  const float ks = I.stress_scale;
+  const float Af00 = ks * tv[0] + mass * C.x, Af01 = ks * tv[1] + mass * C.y;
+  const float Af10 = ks * tv[2] + mass * C.z, Af11 = ks * tv[3] + mass * C.w;
+  const float wx[3] = {st.wx0, st.wx1, st.wx2};
+  const float wy[3] = {st.wy0, st.wy1, st.wy2};
+  const float4* pmb = A.pmbar + I.g_off;
+  float vb0 = 0.f, vb1 = 0.f, Ab00 = 0.f, Ab01 = 0.f, Ab10 = 0.f, Ab11 = 0.f;
+  float xb0 = 0.f, xb1 = 0.f, xa0 = 0.f, xa1 = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float4 pb = pmb[(st.by + j) * I.nx + st.bx + i];
+      const float w = wx[i] * wy[j];
+      const float d0 = ((float)i - st.fx0) * I.dx, d1 = ((float)j - st.fx1) * I.dx;
+      vb0 += w * pb.x;
+      vb1 += w * pb.y;
+      Ab00 += w * pb.x * d0; Ab01 += w * pb.x * d1;
+      Ab10 += w * pb.y * d0; Ab11 += w * pb.y * d1;
+      const float mom0 = mass * v.x + (Af00 * d0 + Af01 * d1);
+      const float mom1 = mass * v.y + (Af10 * d0 + Af11 * d1);
+      const float qv = pb.x * mom0 + pb.y * mom1 + pb.z * mass;
+      xb0 += wd(i, st.fx0) * wy[j] * qv;
+      xb1 += wx[i] * wd(j, st.fx1) * qv;
+      xa0 += w * (Af00 * pb.x + Af10 * pb.y);
+      xa1 += w * (Af01 * pb.x + Af11 * pb.y);
+    }
+  }
+  const float tb[4] = {ks * Ab00, ks * Ab01, ks * Ab10, ks * Ab11};
+  const float4 Fob = A.lF[g];
+  const float fob[4] = {Fob.x, Fob.y, Fob.z, Fob.w};
+  float Fsb[4];
+  if constexpr (kWater) {
+    const float cw = (fob[0] + fob[3]) * kf + (tb[0] + tb[3]) * kt;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) Fsb[e] = cw * dJ[e];
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc += fob[q] * Fo[q].d[e] + tb[q] * tau[q].d[e];
+      Fsb[e] = acc;
+    }
+    if (mt == 3) {
+      *pbar = (tb[0] * fb.x * fb.x + tb[1] * fb.x * fb.y + tb[2] * fb.y * fb.x + tb[3] * fb.y * fb.y) * J.v;
+    }
+  }
+  // F* = M F: F_bar = M^T F*_bar, C_bar += dt F*_bar F^T
+  const float Fb00 = M00 * Fsb[0] + M10 * Fsb[2], Fb01 = M00 * Fsb[1] + M10 * Fsb[3];
+  const float Fb10 = M01 * Fsb[0] + M11 * Fsb[2], Fb11 = M01 * Fsb[1] + M11 * Fsb[3];
+  const float Cb00 = mass * Ab00 + dt * (Fsb[0] * F.x + Fsb[1] * F.y);
+  const float Cb01 = mass * Ab01 + dt * (Fsb[0] * F.z + Fsb[1] * F.w);
+  const float Cb10 = mass * Ab10 + dt * (Fsb[2] * F.x + Fsb[3] * F.y);
+  const float Cb11 = mass * Ab11 + dt * (Fsb[2] * F.z + Fsb[3] * F.w);
+  const float4 lx = make_float4(xt.x + I.inv_dx * xb0 - xa0, xt.y + I.inv_dx * xb1 - xa1, mass * vb0,
+                                mass * vb1);
+  A.lxv[g] = lx;
+  A.lC[g] = make_float4(Cb00, Cb01, Cb10, Cb11);
+  A.lF[g] = make_float4(Fb00, Fb01, Fb10, Fb11);
+  const float chk = ((lx.x + lx.y) + (lx.z + lx.w)) + ((Cb00 + Cb01) + (Cb10 + Cb11)) +
+                    ((Fb00 + Fb01) + (Fb10 + Fb11));
+  if (!isfinite(chk)) atomicOr(a.err + m, 4);
+  return true;
+}
+
+// P2G adjoint of the water particles (most of the tank): the closed-form
+// Jacobian at the register budget of that path; water at the singular-value
+// floor is listed for ad_p2g_list (the full path), and every other material is
+// done by ad_p2g_list over the rollout's list of non-water particles, which
+// runs beside this kernel on a second stream.
+__global__ void __launch_bounds__(kT, 4) ad_p2g_water(AdjArgs A, int32_t* floor_list, int32_t* n_floor) {
   const GradArgs& a = A.f;
   const int m = blockIdx.y;
-  __shared__ double s_fac[3];   // d pressure / d (actuation, contraction, freq)
-  __shared__ double s_sum[kT / 32];
-  if (threadIdx.x == 0) {
-    const JfParams P = a.params[m];
-    const double f = P.freq, c = P.contraction, t = a.t;
-    const float act = jf_activation(P.freq, P.contraction, a.t);
-    const double period = 1.0 / f;
-    const double phase = (t - period * floor(t / period)) / period;
-    double da_dc = 0.0, da_df = 0.0;
-    if (act != 0.0f && phase < c) {
-      const double sn = 0.5 * sin(3.14159265 * phase / c);
-      da_dc = sn * 3.14159265 * (-phase / (c * c));
-      da_df = sn * (3.14159265 / c) * t;
-    }
-    s_fac[0] = act;
-    s_fac[1] = P.actuation * da_dc;
-    s_fac[2] = P.actuation * da_df;
-  }
-  __syncthreads();
-  const float pressure = a.params[m].actuation * (float)s_fac[0];
   const JfInst I = a.inst[m];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  float pbar_p = 0.0f;  // d L / d pressure of this particle
-  if (k < I.n_slots) {
-    const int64_t g = I.p_off + k;
-    const int mt = a.mat[g];
-    if (mt >= 0) {
-      const float4 xv = a.s.xv[g];
-      const float2 x = make_float2(xv.x, xv.y), v = make_float2(xv.z, xv.w);
-      JfStencil st;
-      const float2 xt = A.xtmp[g];
-      if (!jf_stencil_strict(I, x, st)) {
-        A.lxv[g] = make_float4(xt.x, xt.y, A.vtmp[g].x, A.vtmp[g].y);
-        // C and F pass through unchanged outside the stencil range
-      } else {
-        const float4 C = a.s.C[g], F = a.s.F[g];
-        const float4 Fob = A.lF[g];
-        const float dt = I.dt;
-        const float M00 = radd(1.0f, rmul(dt, C.x)), M01 = rmul(dt, C.y);
-        const float M10 = rmul(dt, C.z), M11 = radd(1.0f, rmul(dt, C.w));
-        const float fsv[4] = {rdot2(M00, F.x, M01, F.z), rdot2(M00, F.y, M01, F.w),
-                              rdot2(M10, F.x, M11, F.z), rdot2(M10, F.y, M11, F.w)};
-        const int ms = jf_mat_slot(mt);
-        const JfMaterials& mats = a.mats;
-        const float mu = ms == 0 ? mats.mu[0] : ms == 1 ? mats.mu[1] : ms == 2 ? mats.mu[2]
-                       : ms == 3 ? mats.mu[3] : mats.mu[4];
-        const float la = ms == 0 ? mats.la[0] : ms == 1 ? mats.la[1] : ms == 2 ? mats.la[2]
-                       : ms == 3 ? mats.la[3] : mats.la[4];
-        const float2 fb = (mt == 3) ? a.fiber[g] : make_float2(0.0f, 1.0f);
-        // the material map F* -> (F_out, tau): values and Jacobians d./dF*[e]
-        D4 Fo[4], tau[4], J;
-        const JfSvdRot rot = jf_svd2_values(make_float4(fsv[0], fsv[1], fsv[2], fsv[3]));
-        if (mt == 0 && rot.s1 > 1e-6f && rot.s2 > 1e-6f) {
-          // water, no singular value at the 1e-6 floor: J = s1 s2 = det F*, so
-          // dJ = cof F*; F_out = sqrt(J) I, tau = lambda J (J - 1) I
-          // (mpm_sim.py:219-227 with mu = 0); values as the forward rounds them
-          const float Jw = rmul(rot.s1, rot.s2);
-          const float dJ[4] = {fsv[3], -fsv[2], -fsv[1], fsv[0]};
-          const float kf = 0.5f / sqrtf(Jw), kt = la * (2.0f * Jw - 1.0f);
-          const float sj = sqrtf(Jw), diag = rmul(rmul(la, Jw), rsub(Jw, 1.0f));
-          Fo[0] = d4c(sj); Fo[1] = d4c(0.0f); Fo[2] = d4c(0.0f); Fo[3] = d4c(sj);
-          tau[0] = d4c(diag); tau[1] = d4c(0.0f); tau[2] = d4c(0.0f); tau[3] = d4c(diag);
-          J = d4c(Jw);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            Fo[0].d[e] = Fo[3].d[e] = kf * dJ[e];
-            tau[0].d[e] = tau[3].d[e] = kt * dJ[e];
-            J.d[e] = dJ[e];
-          }
-        } else {
-          D4 Fs[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            Fs[q] = d4c(fsv[q]);
-            Fs[q].d[q] = 1.0f;
-          }
-          jf_phi<D4>(Fs, mt, mu, la, pressure, fb, Fo, tau, J);
-        }
-        float mass = I.p_mass;
-        if (mt == 2) mass = mass * a.params[m].payload_density;
-        const float ks = I.stress_scale;
-        const float Af00 = ks * tau[0].v + mass * C.x, Af01 = ks * tau[1].v + mass * C.y;
-        const float Af10 = ks * tau[2].v + mass * C.z, Af11 = ks * tau[3].v + mass * C.w;
-        const float wx[3] = {st.wx0, st.wx1, st.wx2};
-        const float wy[3] = {st.wy0, st.wy1, st.wy2};
-        const float4* pmb = A.pmbar + I.g_off;
-        float vb0 = 0.f, vb1 = 0.f, Ab00 = 0.f, Ab01 = 0.f, Ab10 = 0.f, Ab11 = 0.f;
-        float xb0 = 0.f, xb1 = 0.f, xa0 = 0.f, xa1 = 0.f;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            const float4 pb = pmb[(st.by + j) * I.nx + st.bx + i];
-            const float w = wx[i] * wy[j];
-            const float d0 = ((float)i - st.fx0) * I.dx, d1 = ((float)j - st.fx1) * I.dx;
-            vb0 += w * pb.x;
-            vb1 += w * pb.y;
-            Ab00 += w * pb.x * d0; Ab01 += w * pb.x * d1;
-            Ab10 += w * pb.y * d0; Ab11 += w * pb.y * d1;
-            const float mom0 = mass * v.x + (Af00 * d0 + Af01 * d1);
-            const float mom1 = mass * v.y + (Af10 * d0 + Af11 * d1);
-            const float qv = pb.x * mom0 + pb.y * mom1 + pb.z * mass;
-            xb0 += wd(i, st.fx0) * wy[j] * qv;
-            xb1 += wx[i] * wd(j, st.fx1) * qv;
-            xa0 += w * (Af00 * pb.x + Af10 * pb.y);
-            xa1 += w * (Af01 * pb.x + Af11 * pb.y);
-          }
-        }
-        const float tb[4] = {ks * Ab00, ks * Ab01, ks * Ab10, ks * Ab11};
-        const float fob[4] = {Fob.x, Fob.y, Fob.z, Fob.w};
-        float Fsb[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          float acc = 0.0f;
-#pragma unroll
-          for (int q = 0; q < 4; ++q) acc += fob[q] * Fo[q].d[e] + tb[q] * tau[q].d[e];
-          Fsb[e] = acc;
-        }
-        if (mt == 3) {
-          pbar_p = (tb[0] * fb.x * fb.x + tb[1] * fb.x * fb.y + tb[2] * fb.y * fb.x + tb[3] * fb.y * fb.y) * J.v;
-        }
-        // F* = M F: F_bar = M^T F*_bar, C_bar += dt F*_bar F^T
-        const float Fb00 = M00 * Fsb[0] + M10 * Fsb[2], Fb01 = M00 * Fsb[1] + M10 * Fsb[3];
-        const float Fb10 = M01 * Fsb[0] + M11 * Fsb[2], Fb11 = M01 * Fsb[1] + M11 * Fsb[3];
-        const float Cb00 = mass * Ab00 + dt * (Fsb[0] * F.x + Fsb[1] * F.y);
-        const float Cb01 = mass * Ab01 + dt * (Fsb[0] * F.z + Fsb[1] * F.w);
-        const float Cb10 = mass * Ab10 + dt * (Fsb[2] * F.x + Fsb[3] * F.y);
-        const float Cb11 = mass * Ab11 + dt * (Fsb[2] * F.z + Fsb[3] * F.w);
-        const float4 lx = make_float4(xt.x + I.inv_dx * xb0 - xa0, xt.y + I.inv_dx * xb1 - xa1, mass * vb0,
-                                      mass * vb1);
-        A.lxv[g] = lx;
-        A.lC[g] = make_float4(Cb00, Cb01, Cb10, Cb11);
-        A.lF[g] = make_float4(Fb00, Fb01, Fb10, Fb11);
-        const float chk = ((lx.x + lx.y) + (lx.z + lx.w)) + ((Cb00 + Cb01) + (Cb10 + Cb11)) +
-                          ((Fb00 + Fb01) + (Fb10 + Fb11));
-        if (!isfinite(chk)) atomicOr(a.err + m, 4);
-      }
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  if (a.mat[g] != 0) return;
+  float pbar;
+  if (!ad_p2g_particle<true>(A, I, m, g, 0, 0.0f, &pbar)) floor_list[atomicAdd(n_floor, 1)] = (int32_t)g;
+}
+
+// P2G adjoint with the full material map (dual-number SVD) over a list of
+// particles; the muscle's d L / d pressure goes into the parameter gradients
+// of its instance.
+__global__ void __launch_bounds__(kT) ad_p2g_list(AdjArgs A, const int32_t* list, const int32_t* n_list,
+                                                  const int32_t* inst_of) {
+  const GradArgs& a = A.f;
+  const int n = *n_list;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int64_t g = list[r];
+    const int m = inst_of[g];
+    const JfInst I = a.inst[m];
+    const double* fm = A.fac + 3 * m;
+    const float pressure = a.params[m].actuation * (float)fm[0];
+    float pbar = 0.0f;
+    ad_p2g_particle<false>(A, I, m, g, a.mat[g], pressure, &pbar);
+    if (pbar != 0.0f) {
+      atomicAdd(A.gparam + 3 * m + 0, (double)pbar * fm[0]);
+      atomicAdd(A.gparam + 3 * m + 1, (double)pbar * fm[1]);
+      atomicAdd(A.gparam + 3 * m + 2, (double)pbar * fm[2]);
+      atomicAdd(A.dLdp + m, (double)pbar);
     }
   }
-  // block sum of d L / d pressure -> parameter gradients of this instance
-  double ps = (double)pbar_p;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) ps += __shfl_down_sync(0xffffffffu, ps, off);
-  if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = ps;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double tot = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_sum[w];
-    if (tot != 0.0) {
-      atomicAdd(A.gparam + 3 * m + 0, tot * s_fac[0]);
-      atomicAdd(A.gparam + 3 * m + 1, tot * s_fac[1]);
-      atomicAdd(A.gparam + 3 * m + 2, tot * s_fac[2]);
-      atomicAdd(A.dLdp + m, tot);
-    }
-  }
+}
+
+// the live particles that are not water (the list ad_p2g_list takes beside
+// the water kernel)
+__global__ void nonwater_list_kernel(const JfInst* __restrict__ inst, const int32_t* __restrict__ mat,
+                                     int32_t* __restrict__ list, int32_t* __restrict__ n) {
+  const int m = blockIdx.y;
+  const JfInst I = inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n_slots) return;
+  const int64_t g = I.p_off + k;
+  if (mat[g] > 0) list[atomicAdd(n, 1)] = (int32_t)g;
 }
 
 // d L / d x at the final state: +1/n on the y of the selected particles
@@ -528,6 +571,14 @@ __global__ void seed_kernel(const JfInst* __restrict__ inst, const int32_t* __re
   }
 }
 
+// instance index of every particle slot
+__global__ void inst_of_kernel(const JfInst* __restrict__ inst, int32_t* __restrict__ out) {
+  const int m = blockIdx.y;
+  const JfInst I = inst[m];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < I.n_slots) out[I.p_off + k] = m;
+}
+
 template <class T>
 cudaError_t alloc_n(T** p, size_t n) {
   return cudaMalloc((void**)p, sizeof(T) * (n > 0 ? n : 1));
@@ -548,14 +599,25 @@ struct JfGrad {
   float4 *lxv = nullptr, *lC = nullptr, *lF = nullptr;
   float2 *xtmp = nullptr, *vtmp = nullptr;
   float4* ck = nullptr;     // n_ck checkpoints x 3 arrays x total slots
-  float4* seg = nullptr;    // K states x 3 arrays x total slots
-  float2* useg = nullptr;   // K grids: updated velocity per node
-  float4* pmseg = nullptr;  // K grids: (momentum x, momentum y, mass) per node
+  // two sets of segment buffers: the backward recomputes segment k - 1 into
+  // one while the adjoint of segment k reads the other
+  float4* seg[2] = {nullptr, nullptr};    // K states x 3 arrays x total slots
+  float2* useg[2] = {nullptr, nullptr};   // K grids: updated velocity per node
+  float4* pmseg[2] = {nullptr, nullptr};  // K grids: (momentum x, momentum y, mass) per node
+  cudaStream_t rstream = nullptr;         // the recompute's stream
+  cudaEvent_t ready[2] = {nullptr, nullptr}, released[2] = {nullptr, nullptr};
   float4* fin = nullptr;    // final state (3 arrays)
   float* fin_Jp = nullptr;  // final Jp (the backward's recompute updates Jp in place)
   double* gparam = nullptr;
   double* dLdp = nullptr;   // steps x M: d L / d pressure per substep and instance
   size_t dLdp_cap = 0;
+  double* fac = nullptr;       // M x 3 pressure factors of the current substep
+  int32_t* solid = nullptr;    // the rollout's non-water live particles
+  int32_t* floor_list = nullptr;  // water at the singular-value floor, per substep
+  int32_t* counts = nullptr;   // [non-water, floor]
+  int32_t* inst_of = nullptr;  // instance of every particle slot
+  cudaStream_t side = nullptr; // second stream of the backward (the non-water P2G adjoint)
+  cudaEvent_t fork = nullptr, join = nullptr;
   int32_t* body_mode = nullptr;
   double* inv_n = nullptr;
   std::vector<double> loss;
@@ -567,8 +629,18 @@ void jf_grad_free(jf_engine* e) {
   if (!G) return;
   cudaFree(G->fix); cudaFree(G->u); cudaFree(G->ubar); cudaFree(G->pmbar);
   cudaFree(G->lxv); cudaFree(G->lC); cudaFree(G->lF); cudaFree(G->xtmp); cudaFree(G->vtmp);
-  cudaFree(G->ck); cudaFree(G->seg); cudaFree(G->useg); cudaFree(G->pmseg); cudaFree(G->fin); cudaFree(G->fin_Jp); cudaFree(G->gparam);
-  cudaFree(G->dLdp);
+  cudaFree(G->ck); cudaFree(G->fin); cudaFree(G->fin_Jp); cudaFree(G->gparam);
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(G->seg[b]); cudaFree(G->useg[b]); cudaFree(G->pmseg[b]);
+    if (G->ready[b]) cudaEventDestroy(G->ready[b]);
+    if (G->released[b]) cudaEventDestroy(G->released[b]);
+  }
+  if (G->rstream) cudaStreamDestroy(G->rstream);
+  cudaFree(G->dLdp); cudaFree(G->fac); cudaFree(G->solid); cudaFree(G->floor_list); cudaFree(G->counts);
+  cudaFree(G->inst_of);
+  if (G->side) cudaStreamDestroy(G->side);
+  if (G->fork) cudaEventDestroy(G->fork);
+  if (G->join) cudaEventDestroy(G->join);
   cudaFree(G->body_mode); cudaFree(G->inv_n);
   delete G;
   e->grad = nullptr;
@@ -598,19 +670,22 @@ static GradState state_at(float4* base, size_t slots, size_t idx) {
   return GradState{b, b + slots, b + 2 * slots};
 }
 
-static cudaError_t copy_state(jf_engine* e, GradState dst, GradState src) {
+static cudaError_t copy_state(jf_engine* e, GradState dst, GradState src, cudaStream_t st = nullptr) {
   const size_t bytes = sizeof(float4) * (size_t)e->total_slots;
+  if (!st) st = e->stream;
   cudaError_t err;
-  if ((err = cudaMemcpyAsync(dst.xv, src.xv, bytes, cudaMemcpyDeviceToDevice, e->stream)) != cudaSuccess) return err;
-  if ((err = cudaMemcpyAsync(dst.C, src.C, bytes, cudaMemcpyDeviceToDevice, e->stream)) != cudaSuccess) return err;
-  return cudaMemcpyAsync(dst.F, src.F, bytes, cudaMemcpyDeviceToDevice, e->stream);
+  if ((err = cudaMemcpyAsync(dst.xv, src.xv, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return err;
+  if ((err = cudaMemcpyAsync(dst.C, src.C, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return err;
+  return cudaMemcpyAsync(dst.F, src.F, bytes, cudaMemcpyDeviceToDevice, st);
 }
 
 // one deterministic substep of every instance from state s at time t into
 // state o (s itself when o is not given); with u_keep / pmv_keep set, its grid
 // is written there for the adjoint
 static cudaError_t det_substep(jf_engine* e, GradState s, float t, float2* u_keep = nullptr,
-                               float4* pmv_keep = nullptr, const GradState* o = nullptr) {
+                               float4* pmv_keep = nullptr, const GradState* o = nullptr,
+                               cudaStream_t st = nullptr) {
+  if (!st) st = e->stream;
   JfGrad* G = e->grad;
   GradArgs a = grad_args(e, s, t);
   if (o) a.o = *o;
@@ -618,12 +693,12 @@ static cudaError_t det_substep(jf_engine* e, GradState s, float t, float2* u_kee
     a.u = u_keep;
     a.pmv = pmv_keep;
   }
-  cudaError_t err = cudaMemsetAsync(G->fix, 0, sizeof(unsigned long long) * 3 * (size_t)e->total_nodes, e->stream);
+  cudaError_t err = cudaMemsetAsync(G->fix, 0, sizeof(unsigned long long) * 3 * (size_t)e->total_nodes, st);
   if (err != cudaSuccess) return err;
   const dim3 gp((e->max_slots + kT - 1) / kT, e->M), gn((e->max_cells + kT - 1) / kT, e->M);
-  gf_p2g<<<gp, kT, 0, e->stream>>>(a);
-  gf_grid<<<gn, kT, 0, e->stream>>>(a);
-  gf_g2p<<<gp, kT, 0, e->stream>>>(a);
+  gf_p2g<<<gp, kT, 0, st>>>(a);
+  gf_grid<<<gn, kT, 0, st>>>(a);
+  gf_g2p<<<gp, kT, 0, st>>>(a);
   e->launches += 3;
   return cudaGetLastError();
 }
@@ -650,6 +725,22 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
     if ((err = alloc_n(&G->gparam, 3 * (size_t)e->M)) != cudaSuccess) return err;
     if ((err = alloc_n(&G->body_mode, e->M)) != cudaSuccess) return err;
     if ((err = alloc_n(&G->inv_n, e->M)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->fac, 3 * (size_t)e->M)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->solid, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->floor_list, slots)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->counts, 2)) != cudaSuccess) return err;
+    if ((err = alloc_n(&G->inst_of, slots)) != cudaSuccess) return err;
+    if ((err = cudaStreamCreateWithFlags(&G->side, cudaStreamNonBlocking)) != cudaSuccess) return err;
+    if ((err = cudaEventCreateWithFlags(&G->fork, cudaEventDisableTiming)) != cudaSuccess) return err;
+    if ((err = cudaEventCreateWithFlags(&G->join, cudaEventDisableTiming)) != cudaSuccess) return err;
+    if ((err = cudaStreamCreateWithFlags(&G->rstream, cudaStreamNonBlocking)) != cudaSuccess) return err;
+    for (int b = 0; b < 2; ++b) {
+      if ((err = cudaEventCreateWithFlags(&G->ready[b], cudaEventDisableTiming)) != cudaSuccess) return err;
+      if ((err = cudaEventCreateWithFlags(&G->released[b], cudaEventDisableTiming)) != cudaSuccess) return err;
+    }
+    const dim3 gp((e->max_slots + kT - 1) / kT, e->M);
+    inst_of_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, G->inst_of);
+    e->launches += 1;
   }
   if (G->n_ck < n_ck) {
     cudaFree(G->ck);
@@ -671,6 +762,13 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
   G->steps = steps;
   G->K = K;
   G->t0 = e->t;
+  // the rollout's non-water particles, for the backward's second stream
+  if ((err = cudaMemsetAsync(G->counts, 0, sizeof(int32_t), e->stream))) return err;
+  {
+    const dim3 gp((e->max_slots + kT - 1) / kT, e->M);
+    nonwater_list_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, e->p.mat, G->solid, G->counts);
+    e->launches += 1;
+  }
   const GradState work{e->p.xv, e->p.C, e->p.F};
   const float dtf = (float)e->dt;
   float t = e->t;
@@ -749,38 +847,63 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   // the segment buffers (K pre-step states and grids) are needed only here,
   // so a forward-only rollout does not hold them
   if (G->seg_cap < (size_t)K) {
-    cudaFree(G->seg);
-    cudaFree(G->useg);
-    cudaFree(G->pmseg);
-    G->seg = nullptr;
-    G->useg = nullptr;
-    G->pmseg = nullptr;
     G->seg_cap = 0;
-    if ((err = alloc_n(&G->seg, 3 * slots * (size_t)K)) != cudaSuccess) return err;
-    if ((err = alloc_n(&G->useg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
-    if ((err = alloc_n(&G->pmseg, (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(G->seg[b]);
+      cudaFree(G->useg[b]);
+      cudaFree(G->pmseg[b]);
+      G->seg[b] = nullptr;
+      G->useg[b] = nullptr;
+      G->pmseg[b] = nullptr;
+      if ((err = alloc_n(&G->seg[b], 3 * slots * (size_t)K)) != cudaSuccess) return err;
+      if ((err = alloc_n(&G->useg[b], (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+      if ((err = alloc_n(&G->pmseg[b], (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+    }
     G->seg_cap = (size_t)K;
   }
   const GradState work{e->p.xv, e->p.C, e->p.F};
   const int64_t n_seg = (steps + K - 1) / K;
-  for (int64_t seg = n_seg - 1; seg >= 0; --seg) {
-    const int64_t s0 = seg * K;
-    const int n = (int)((steps - s0) < K ? (steps - s0) : K);
-    // the segment's pre-step states: substep j reads seg[j] and writes seg[j + 1]
-    if ((err = copy_state(e, state_at(G->seg, slots, 0), state_at(G->ck, slots, (size_t)seg))) != cudaSuccess)
-      return err;
-    const size_t nodes = (size_t)e->total_nodes;
+  const size_t nodes = (size_t)e->total_nodes;
+  int n_sm = 148;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, e->device);
+  const int list_blocks = 2 * n_sm;  // grid-stride over the listed particles
+  const int floor_blocks = 16;       // water at the singular-value floor: rare
+  auto seg_len = [&](int64_t seg) { return (int)((steps - seg * K) < K ? (steps - seg * K) : K); };
+  // Recompute of segment `seg` into buffer set b on the recompute stream: its
+  // pre-step states (substep j reads state j and writes state j + 1; the last
+  // writes the engine's work arrays, which nothing reads) and every substep's
+  // grid.  It waits until the adjoint that last read buffer set b is done.
+  // The recompute needs only its checkpoint, so it runs while the main stream
+  // runs the adjoint of the segment after it.
+  auto recompute = [&](int64_t seg, int b) -> cudaError_t {
+    cudaError_t r;
+    if ((r = cudaStreamWaitEvent(G->rstream, G->released[b], 0))) return r;
+    if ((r = copy_state(e, state_at(G->seg[b], slots, 0), state_at(G->ck, slots, (size_t)seg), G->rstream)))
+      return r;
+    const int n = seg_len(seg);
     for (int j = 0; j < n; ++j) {
-      JfTimed timed(e, true);
-      const GradState next = (j + 1 < n) ? state_at(G->seg, slots, (size_t)j + 1) : work;
-      if ((err = det_substep(e, state_at(G->seg, slots, (size_t)j), ts[s0 + j], G->useg + nodes * j,
-                             G->pmseg + nodes * j, &next)) != cudaSuccess)
-        return err;
+      const GradState next = (j + 1 < n) ? state_at(G->seg[b], slots, (size_t)j + 1) : work;
+      if ((r = det_substep(e, state_at(G->seg[b], slots, (size_t)j), ts[seg * K + j], G->useg[b] + nodes * j,
+                           G->pmseg[b] + nodes * j, &next, G->rstream)))
+        return r;
     }
+    return cudaEventRecord(G->ready[b], G->rstream);
+  };
+  // the recompute stream starts after everything queued on the main stream
+  // (the forward's state and the seeds above)
+  if ((err = cudaEventRecord(G->released[0], e->stream))) return err;
+  if ((err = cudaEventRecord(G->released[1], e->stream))) return err;
+  if ((err = recompute(n_seg - 1, 0))) return err;
+  for (int64_t seg = n_seg - 1; seg >= 0; --seg) {
+    const int b = (int)((n_seg - 1 - seg) & 1);
+    if (seg > 0 && (err = recompute(seg - 1, b ^ 1))) return err;
+    if ((err = cudaStreamWaitEvent(e->stream, G->ready[b], 0))) return err;
+    const int64_t s0 = seg * K;
+    const int n = seg_len(seg);
     for (int j = n - 1; j >= 0; --j) {
       JfTimed timed(e, false);
       AdjArgs A;
-      A.f = grad_args(e, state_at(G->seg, slots, (size_t)j), ts[s0 + j]);
+      A.f = grad_args(e, state_at(G->seg[b], slots, (size_t)j), ts[s0 + j]);
       A.lxv = G->lxv;
       A.lC = G->lC;
       A.lF = G->lF;
@@ -790,16 +913,26 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
       A.vtmp = G->vtmp;
       A.gparam = G->gparam;
       A.dLdp = G->dLdp + (size_t)(s0 + j) * e->M;
+      A.fac = G->fac;
       // the substep's grid as the recompute left it
-      A.f.u = G->useg + nodes * j;
-      A.f.pmv = G->pmseg + nodes * j;
+      A.f.u = G->useg[b] + nodes * j;
+      A.f.pmv = G->pmseg[b] + nodes * j;
       if ((err = cudaMemsetAsync(G->ubar, 0, sizeof(float2) * nodes, e->stream))) return err;
+      if ((err = cudaMemsetAsync(G->counts + 1, 0, sizeof(int32_t), e->stream))) return err;
       ad_g2p<<<gp, kT, 0, e->stream>>>(A);
       ad_grid<<<gn, kT, 0, e->stream>>>(A);
-      ad_p2g<<<gp, kT, 0, e->stream>>>(A);
-      e->launches += 3;
+      // P2G adjoint: the non-water particles on the second stream, beside the water
+      if ((err = cudaEventRecord(G->fork, e->stream))) return err;
+      if ((err = cudaStreamWaitEvent(G->side, G->fork, 0))) return err;
+      ad_p2g_list<<<list_blocks, kT, 0, G->side>>>(A, G->solid, G->counts, G->inst_of);
+      if ((err = cudaEventRecord(G->join, G->side))) return err;
+      ad_p2g_water<<<gp, kT, 0, e->stream>>>(A, G->floor_list, G->counts + 1);
+      ad_p2g_list<<<floor_blocks, kT, 0, e->stream>>>(A, G->floor_list, G->counts + 1, G->inst_of);
+      if ((err = cudaStreamWaitEvent(e->stream, G->join, 0))) return err;
+      e->launches += 5;
       if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
+    if ((err = cudaEventRecord(G->released[b], e->stream))) return err;
   }
   // the initial CoM term of the displacement
   seed_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, e->p.mat, G->body_mode, G->inv_n, G->lxv, G->lC, G->lF, 0, -1.0f);

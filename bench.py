@@ -239,13 +239,15 @@ def uneven_leg(device, stream, substeps=5000):
     return out
 
 
-def refine_leg(device, stream, M=256, steps=400, iterations=3, checkpoint_every=50):
+def refine_leg(device, stream, M=256, steps=4000, iterations=3, checkpoint_every=50):
     """The gradient-refined search step of the 256 x 64^2 configuration (dx = 1/64,
-    20,000 slots, ~14.9K live), on a bounded sample of its 4,000-substep horizon:
-    genomes from a seeded Gaussian (CMA-ES style) sample, `iterations` gradient
-    steps of 0.05 of the range on the two timing genes (each a checkpointed
-    forward + backward of all instances), then the initial and refined genomes
-    re-evaluated by the plain forward path and the GPU fitness kernel."""
+    20,000 slots, ~14.9K live) over its 4,000-substep horizon: genomes from a
+    seeded Gaussian (CMA-ES style) sample, `iterations` gradient steps of 0.05
+    of the range on the two timing genes (each the checkpointed forward and
+    the backward of all instances replayed as one CUDA graph), then the
+    initial and refined genomes re-evaluated by the plain forward path and the
+    GPU fitness kernel.  The first iteration of an untimed warm-up run
+    captures the graph."""
     import torch
     from jellyfih_b200 import Engine, InstanceSpec, tank
     from jellyfih_b200.autograd import refine_timing_genes
@@ -258,7 +260,7 @@ def refine_leg(device, stream, M=256, steps=400, iterations=3, checkpoint_every=
     spec = InstanceSpec(20000, 64, 64, 1.0)
     e = Engine([spec] * M, path="plain", device=device)
     e.set_stream(stream)
-    refine_timing_genes(e, genomes, pos, mats, fibs, steps, 1, checkpoint_every=checkpoint_every)  # warm-up
+    refine_timing_genes(e, genomes, pos, mats, fibs, steps, 1, checkpoint_every=checkpoint_every)  # warm-up, capture
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     refined, hist = refine_timing_genes(e, genomes, pos, mats, fibs, steps, iterations,

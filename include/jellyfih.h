@@ -173,6 +173,16 @@ int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, cons
 int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss);
 int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, double* d_freq);
 int jf_grad_positions(jf_engine* e, int32_t m, float* dx0);
+/* jf_grad_forward followed by jf_grad_backward with one host round trip
+ * between none of their device work: both run as one CUDA graph, captured on
+ * the first call and replayed while the sizes, start time and buffers are
+ * unchanged (the gradient-refinement loop: every step restarts from time 0).
+ * jf_grad_forward / jf_grad_backward each replay a graph of their own the
+ * same way.  With JF_FLAG_NO_GRAPHS, or while kernel timing is on, the work
+ * is launched directly.  Outputs as the two calls'; jf_grad_positions works
+ * after it. */
+int jf_grad_step(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss, double* d_actuation,
+                 double* d_contraction, double* d_freq);
 
 /* Particle fields of instance m in slot order (field.to_numpy()); any
  * pointer may be NULL.  x, v, fiber: [n_slots][2]; C, F: [n_slots][4]. */

@@ -65,6 +65,7 @@ EXPORTS = {
     "jf_grad_forward": (ctypes.c_int, [_E, ctypes.c_int64, ctypes.c_int32, _P]),
     "jf_grad_backward": (ctypes.c_int, [_E, _P, _P, _P]),
     "jf_grad_positions": (ctypes.c_int, [_E, ctypes.c_int32, _P]),
+    "jf_grad_step": (ctypes.c_int, [_E, ctypes.c_int64, ctypes.c_int32, _P, _P, _P, _P]),
     "jf_read_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "jf_write_particles": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P, _P, _P, _P, _P]),
     "jf_read_grid": (ctypes.c_int, [_E, ctypes.c_int32, _P, _P]),

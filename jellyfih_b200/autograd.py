@@ -6,7 +6,8 @@ loads every instance from `positions`, runs `steps` substeps with checkpoints
 its backward calls the hand-written adjoint kernels (jf_grad_backward,
 jf_grad_positions).  `refine_timing_genes` takes gradient steps on the two
 actuation-timing genes (contraction fraction, frequency multiplier) beside
-CMA-ES, as an optional refinement.
+CMA-ES, as an optional refinement, each step's forward and backward replayed
+as one CUDA graph (jf_grad_step).
 """
 from __future__ import annotations
 
@@ -62,27 +63,32 @@ def refine_timing_genes(engine, genomes, positions, materials, fibers, steps, it
                         step_frac=0.05, actuation=500.0, checkpoint_every=100):
     """Gradient steps on genes 9 (contraction) and 10 (frequency multiplier).
 
-    Each iteration moves each gene by step_frac of its range in the direction
-    that raises the payload's displacement, clipped to the gene bounds
-    (evolve.py:55-62).  An instance whose rollout or adjoint went non-finite
-    (the engine's error flags) keeps its genes for that iteration.  Returns
-    the refined genomes and the displacement before every step.
+    Each iteration loads every instance's initial particles, runs the
+    checkpointed forward and the backward of all instances as one CUDA graph
+    (Engine.grad_step; the graph is captured on the first iteration and
+    replayed after), and moves each gene by step_frac of its range in the
+    direction that raises the payload's displacement, clipped to the gene
+    bounds (evolve.py:55-62).  An instance whose rollout or adjoint went
+    non-finite (the engine's error flags) keeps its genes for that iteration.
+    Returns the refined genomes and the displacement before every step.
     """
     g = np.array(genomes, dtype=np.float64, copy=True)
     M = len(g)
-    pos = torch.as_tensor(np.stack(positions), dtype=torch.float32)
     history = []
     for _ in range(iterations):
         engine.clear_error_flags()
-        c = torch.tensor(np.clip(g[:, 9], 0.05, 0.60), dtype=torch.float64, requires_grad=True)
-        f = torch.tensor(np.clip(g[:, 10], 0.5, 2.0), dtype=torch.float64, requires_grad=True)
-        a = torch.full((M,), actuation, dtype=torch.float64)
-        disp = rollout_displacement(engine, a, c, f, pos, materials, fibers, steps, checkpoint_every)
-        disp.sum().backward()
-        history.append(disp.detach().numpy().copy())
+        c = np.clip(g[:, 9], 0.05, 0.60)
+        f = np.clip(g[:, 10], 0.5, 2.0)
+        engine.set_params(actuation=np.full(M, actuation, np.float32), contraction=c.astype(np.float32),
+                          freq=f.astype(np.float32))
+        for m in range(M):
+            engine.load(m, positions[m], materials[m], fibers[m])
+        engine.time = 0.0
+        disp, grads = engine.grad_step(int(steps), int(checkpoint_every))
+        history.append(disp.copy())
         ok = engine.error_flags() == 0
-        for k, grad in ((9, c.grad), (10, f.grad)):
+        for k, name in ((9, "contraction"), (10, "freq")):
             span = GENOME_UPPER[k] - GENOME_LOWER[k]
-            step = np.where(ok, step_frac * span * np.sign(np.nan_to_num(grad.numpy())), 0.0)
+            step = np.where(ok, step_frac * span * np.sign(np.nan_to_num(grads[name])), 0.0)
             g[:, k] = np.clip(g[:, k] + step, GENOME_LOWER[k], GENOME_UPPER[k])
     return g, history

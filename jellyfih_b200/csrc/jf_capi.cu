@@ -770,31 +770,36 @@ int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, cons
   return nonfinite_status(e, flags);
 }
 
-int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss) {
-  if (check_engine(e)) return JF_ERR_INVALID;
-  if (steps <= 0 || checkpoint_every <= 0) return fail(e, JF_ERR_INVALID, "steps and checkpoint_every must be > 0");
-  if (e->flags & JF_FLAG_AXISYM)
-    return fail(e, JF_ERR_UNSUPPORTED, "the differentiable rollout has no axisymmetric variant");
-  int rc = set_device(e);
+// The CoM each instance's loss follows (payload; jelly + muscle without
+// payload, mpm_sim.py:786-792) from the current state: selection, 1 / count
+// and the initial height.
+static int grad_prologue(jf_engine* e, std::vector<int32_t>& body, std::vector<double>& inv_n,
+                         std::vector<double>& init) {
+  int rc = upload_params(e);
   if (rc) return rc;
-  if ((rc = upload_params(e))) return rc;
   std::vector<double> raw(6 * (size_t)e->M);
   JF_CK(jf_stats_launch(e), "stats kernel");
   JF_CK(cudaMemcpyAsync(raw.data(), e->d_stats, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, e->stream),
         "read stats");
   JF_CK(cudaStreamSynchronize(e->stream), "stats sync");
-  std::vector<int32_t> body(e->M);
-  std::vector<double> inv_n(e->M), init(e->M);
+  body.assign(e->M, 0);
+  inv_n.assign(e->M, 0.0);
+  init.assign(e->M, 0.0);
   for (int m = 0; m < e->M; ++m) {
     const double* r = &raw[6 * (size_t)m];
-    body[m] = r[1] == 0 ? 1 : 0;  // no payload: the jelly + muscle CoM (mpm_sim.py:786-792)
+    body[m] = r[1] == 0 ? 1 : 0;
     const double cnt = body[m] ? r[4] : r[1];
     const double sy = body[m] ? r[3] : r[0];
     inv_n[m] = cnt > 0 ? 1.0 / cnt : 0.0;
     init[m] = cnt > 0 ? sy / cnt : 0.0;
   }
-  JF_CK(jf_grad_forward_impl(e, steps, checkpoint_every, body.data(), inv_n.data()), "gradient forward");
-  JF_CK(jf_stats_launch(e), "stats kernel");
+  return JF_OK;
+}
+
+// loss[m] = final CoM height - initial, from the sums in e->d_stats
+static int grad_loss(jf_engine* e, const std::vector<int32_t>& body, const std::vector<double>& init,
+                     double* loss) {
+  std::vector<double> raw(6 * (size_t)e->M);
   JF_CK(cudaMemcpyAsync(raw.data(), e->d_stats, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, e->stream),
         "read stats");
   JF_CK(cudaStreamSynchronize(e->stream), "stats sync");
@@ -804,6 +809,50 @@ int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, doubl
     const double sy = body[m] ? r[3] : r[0];
     const double fin = cnt > 0 ? sy / cnt : 0.0;
     if (loss) loss[m] = fin - init[m];
+  }
+  return JF_OK;
+}
+
+static int grad_check_args(jf_engine* e, int64_t steps, int32_t checkpoint_every) {
+  if (steps <= 0 || checkpoint_every <= 0) return fail(e, JF_ERR_INVALID, "steps and checkpoint_every must be > 0");
+  if (e->flags & JF_FLAG_AXISYM)
+    return fail(e, JF_ERR_UNSUPPORTED, "the differentiable rollout has no axisymmetric variant");
+  return JF_OK;
+}
+
+int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = grad_check_args(e, steps, checkpoint_every);
+  if (rc) return rc;
+  if ((rc = set_device(e))) return rc;
+  std::vector<int32_t> body;
+  std::vector<double> inv_n, init;
+  if ((rc = grad_prologue(e, body, inv_n, init))) return rc;
+  JF_CK(jf_grad_forward_impl(e, steps, checkpoint_every, body.data(), inv_n.data()), "gradient forward");
+  JF_CK(jf_stats_launch(e), "stats kernel");
+  if ((rc = grad_loss(e, body, init, loss))) return rc;
+  e->sorted = false;
+  std::vector<int32_t> flags;
+  if ((rc = read_flags_and_sync(e, flags))) return rc;
+  return nonfinite_status(e, flags);
+}
+
+int jf_grad_step(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss, double* d_actuation,
+                 double* d_contraction, double* d_freq) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  int rc = grad_check_args(e, steps, checkpoint_every);
+  if (rc) return rc;
+  if ((rc = set_device(e))) return rc;
+  std::vector<int32_t> body;
+  std::vector<double> inv_n, init;
+  if ((rc = grad_prologue(e, body, inv_n, init))) return rc;
+  std::vector<double> g(3 * (size_t)e->M);
+  JF_CK(jf_grad_step_impl(e, steps, checkpoint_every, body.data(), inv_n.data(), g.data()), "gradient step");
+  if ((rc = grad_loss(e, body, init, loss))) return rc;
+  for (int m = 0; m < e->M; ++m) {
+    if (d_actuation) d_actuation[m] = g[3 * (size_t)m + 0];
+    if (d_contraction) d_contraction[m] = g[3 * (size_t)m + 1];
+    if (d_freq) d_freq[m] = g[3 * (size_t)m + 2];
   }
   e->sorted = false;
   std::vector<int32_t> flags;

@@ -150,6 +150,8 @@ cudaError_t jf_fitness_launch(jf_engine* e, const double* d_rows, const int32_t*
 cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
                                  const double* inv_n);
 cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host);
+cudaError_t jf_grad_step_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
+                              const double* inv_n, double* gparam_host);
 cudaError_t jf_grad_x0_impl(jf_engine* e, int m, std::vector<float4>& out);
 void jf_grad_free(jf_engine* e);
 

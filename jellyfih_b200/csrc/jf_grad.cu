@@ -37,6 +37,7 @@
 // stencil, the node contributions and the G2P gather in the reference's node
 // order), so that, apart from the order-free fixed-point P2G sums, it performs
 // the reference's FP32 arithmetic exactly.
+#include <cstring>
 #include <vector>
 
 #include "jf_dual.cuh"
@@ -586,6 +587,14 @@ cudaError_t alloc_n(T** p, size_t n) {
 
 }  // namespace
 
+// A CUDA graph of a rollout's device work, replayed while its key (sizes,
+// start time, buffer addresses) is unchanged.
+struct GradGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<uint64_t> key;
+  int64_t launches = 0;  // kernels one replay launches
+};
+
 // Device buffers of the differentiable rollout, owned by the engine.
 struct JfGrad {
   int64_t steps = 0;
@@ -622,6 +631,8 @@ struct JfGrad {
   double* inv_n = nullptr;
   std::vector<double> loss;
   bool have_forward = false;
+  int n_sm = 148;
+  GradGraph fwd_graph, bwd_graph, step_graph;  // forward, backward, forward + backward
 };
 
 void jf_grad_free(jf_engine* e) {
@@ -636,6 +647,8 @@ void jf_grad_free(jf_engine* e) {
     if (G->released[b]) cudaEventDestroy(G->released[b]);
   }
   if (G->rstream) cudaStreamDestroy(G->rstream);
+  for (GradGraph* gg : {&G->fwd_graph, &G->bwd_graph, &G->step_graph})
+    if (gg->exec) cudaGraphExecDestroy(gg->exec);
   cudaFree(G->dLdp); cudaFree(G->fac); cudaFree(G->solid); cudaFree(G->floor_list); cudaFree(G->counts);
   cudaFree(G->inst_of);
   if (G->side) cudaStreamDestroy(G->side);
@@ -703,8 +716,9 @@ static cudaError_t det_substep(jf_engine* e, GradState s, float t, float2* u_kee
   return cudaGetLastError();
 }
 
-cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
-                                 const double* inv_n) {
+// Every buffer of a rollout of `steps` substeps with a checkpoint every K
+// (allocated before any graph capture: capture allows no allocation).
+static cudaError_t grad_alloc(jf_engine* e, int64_t steps, int32_t K) {
   if (!e->grad) e->grad = new JfGrad();
   JfGrad* G = e->grad;
   const size_t slots = (size_t)e->total_slots;
@@ -741,6 +755,7 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
     const dim3 gp((e->max_slots + kT - 1) / kT, e->M);
     inst_of_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, G->inst_of);
     e->launches += 1;
+    cudaDeviceGetAttribute(&G->n_sm, cudaDevAttrMultiProcessorCount, e->device);
   }
   if (G->n_ck < n_ck) {
     cudaFree(G->ck);
@@ -755,13 +770,33 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
     if ((err = alloc_n(&G->dLdp, (size_t)steps * e->M)) != cudaSuccess) return err;
     G->dLdp_cap = (size_t)steps * e->M;
   }
-  if ((err = cudaMemcpyAsync(G->body_mode, body_mode, sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream)))
-    return err;
-  if ((err = cudaMemcpyAsync(G->inv_n, inv_n, sizeof(double) * e->M, cudaMemcpyHostToDevice, e->stream)))
-    return err;
-  G->steps = steps;
-  G->K = K;
-  G->t0 = e->t;
+  // the segment buffers of the backward (K pre-step states and grids, two sets)
+  if (G->seg_cap < (size_t)K) {
+    G->seg_cap = 0;
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(G->seg[b]);
+      cudaFree(G->useg[b]);
+      cudaFree(G->pmseg[b]);
+      G->seg[b] = nullptr;
+      G->useg[b] = nullptr;
+      G->pmseg[b] = nullptr;
+      if ((err = alloc_n(&G->seg[b], 3 * slots * (size_t)K)) != cudaSuccess) return err;
+      if ((err = alloc_n(&G->useg[b], (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+      if ((err = alloc_n(&G->pmseg[b], (size_t)e->total_nodes * K)) != cudaSuccess) return err;
+    }
+    G->seg_cap = (size_t)K;
+  }
+  return cudaSuccess;
+}
+
+// The forward's device work: the non-water list, the substeps from G->t0
+// with their checkpoints, and copies of the final state.
+static cudaError_t fwd_record(jf_engine* e) {
+  JfGrad* G = e->grad;
+  const size_t slots = (size_t)e->total_slots;
+  const int64_t steps = G->steps;
+  const int32_t K = G->K;
+  cudaError_t err;
   // the rollout's non-water particles, for the backward's second stream
   if ((err = cudaMemsetAsync(G->counts, 0, sizeof(int32_t), e->stream))) return err;
   {
@@ -771,7 +806,7 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
   }
   const GradState work{e->p.xv, e->p.C, e->p.F};
   const float dtf = (float)e->dt;
-  float t = e->t;
+  float t = G->t0;
   for (int64_t s = 0; s < steps; ++s) {
     if (s % K == 0) {
       if ((err = copy_state(e, state_at(G->ck, slots, s / K), work)) != cudaSuccess) return err;
@@ -782,12 +817,8 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
     }
     t = t + dtf;
   }
-  e->t = t;
   if ((err = copy_state(e, state_at(G->fin, slots, 0), work)) != cudaSuccess) return err;
-  if ((err = cudaMemcpyAsync(G->fin_Jp, e->p.Jp, sizeof(float) * slots, cudaMemcpyDeviceToDevice, e->stream)))
-    return err;
-  G->have_forward = true;
-  return cudaSuccess;
+  return cudaMemcpyAsync(G->fin_Jp, e->p.Jp, sizeof(float) * slots, cudaMemcpyDeviceToDevice, e->stream);
 }
 
 // Phase of the waveform at time t in FP32, as jf_activation computes it
@@ -829,7 +860,11 @@ static void add_waveform_drop_terms(const jf_engine* e, const std::vector<float>
   }
 }
 
-cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
+// The backward's device work: seeds, the recompute of every segment (on its
+// own stream, overlapped with the adjoint of the segment after it), the
+// adjoint substeps in reverse, and the engine's state restored to the
+// forward's final state.
+static cudaError_t bwd_record(jf_engine* e) {
   JfGrad* G = e->grad;
   const size_t slots = (size_t)e->total_slots;
   const int64_t steps = G->steps;
@@ -844,29 +879,10 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   if ((err = cudaMemsetAsync(G->dLdp, 0, sizeof(double) * (size_t)steps * e->M, e->stream))) return err;
   seed_kernel<<<gp, kT, 0, e->stream>>>(e->d_inst, e->p.mat, G->body_mode, G->inv_n, G->lxv, G->lC, G->lF, 1, 1.0f);
   e->launches += 1;
-  // the segment buffers (K pre-step states and grids) are needed only here,
-  // so a forward-only rollout does not hold them
-  if (G->seg_cap < (size_t)K) {
-    G->seg_cap = 0;
-    for (int b = 0; b < 2; ++b) {
-      cudaFree(G->seg[b]);
-      cudaFree(G->useg[b]);
-      cudaFree(G->pmseg[b]);
-      G->seg[b] = nullptr;
-      G->useg[b] = nullptr;
-      G->pmseg[b] = nullptr;
-      if ((err = alloc_n(&G->seg[b], 3 * slots * (size_t)K)) != cudaSuccess) return err;
-      if ((err = alloc_n(&G->useg[b], (size_t)e->total_nodes * K)) != cudaSuccess) return err;
-      if ((err = alloc_n(&G->pmseg[b], (size_t)e->total_nodes * K)) != cudaSuccess) return err;
-    }
-    G->seg_cap = (size_t)K;
-  }
   const GradState work{e->p.xv, e->p.C, e->p.F};
   const int64_t n_seg = (steps + K - 1) / K;
   const size_t nodes = (size_t)e->total_nodes;
-  int n_sm = 148;
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, e->device);
-  const int list_blocks = 2 * n_sm;  // grid-stride over the listed particles
+  const int list_blocks = 2 * G->n_sm;  // grid-stride over the listed particles
   const int floor_blocks = 16;       // water at the singular-value floor: rare
   auto seg_len = [&](int64_t seg) { return (int)((steps - seg * K) < K ? (steps - seg * K) : K); };
   // Recompute of segment `seg` into buffer set b on the recompute stream: its
@@ -941,6 +957,19 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   if ((err = copy_state(e, work, state_at(G->fin, slots, 0))) != cudaSuccess) return err;
   if ((err = cudaMemcpyAsync(e->p.Jp, G->fin_Jp, sizeof(float) * slots, cudaMemcpyDeviceToDevice, e->stream)))
     return err;
+  return cudaSuccess;
+}
+
+// After the backward's device work: the parameter gradients and the
+// per-substep d L / d pressure to the host, then the waveform-drop terms.
+static cudaError_t bwd_finish(jf_engine* e, double* gparam_host) {
+  JfGrad* G = e->grad;
+  const int64_t steps = G->steps;
+  const float dtf = (float)e->dt;
+  std::vector<float> ts((size_t)steps + 1);
+  ts[0] = G->t0;
+  for (int64_t s = 0; s < steps; ++s) ts[s + 1] = ts[s] + dtf;
+  cudaError_t err;
   if ((err = cudaMemcpyAsync(gparam_host, G->gparam, sizeof(double) * 3 * e->M, cudaMemcpyDeviceToHost, e->stream)))
     return err;
   std::vector<double> dLdp((size_t)steps * e->M);
@@ -950,6 +979,106 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
   if ((err = cudaStreamSynchronize(e->stream))) return err;
   add_waveform_drop_terms(e, ts, dLdp, gparam_host);
   return cudaSuccess;
+}
+
+// Runs `record` (device work on the engine's stream) directly, or, with
+// graphs on and per-kernel timing off, from a CUDA graph captured on first
+// use and replayed while `key` is unchanged.
+template <class Record>
+static cudaError_t run_graph(jf_engine* e, GradGraph& gg, const std::vector<uint64_t>& key, Record record) {
+  if (!e->use_graphs || e->timing) return record();
+  if (!gg.exec || gg.key != key) {
+    if (gg.exec) {
+      cudaGraphExecDestroy(gg.exec);
+      gg.exec = nullptr;
+    }
+    const int64_t launches = e->launches;
+    cudaGraph_t graph = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return err;
+    e->capturing = true;
+    const cudaError_t rec = record();
+    e->capturing = false;
+    err = cudaStreamEndCapture(e->stream, &graph);
+    gg.launches = e->launches - launches;
+    e->launches = launches;  // nothing ran yet
+    if (rec != cudaSuccess || err != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return rec != cudaSuccess ? rec : err;
+    }
+    err = cudaGraphInstantiate(&gg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return err;
+    gg.key = key;
+  }
+  e->launches += gg.launches;
+  return cudaGraphLaunch(gg.exec, e->stream);
+}
+
+static std::vector<uint64_t> graph_key(const jf_engine* e, int tag) {
+  const JfGrad* G = e->grad;
+  uint32_t tbits;
+  memcpy(&tbits, &G->t0, sizeof(tbits));
+  return {(uint64_t)tag, (uint64_t)G->steps, (uint64_t)G->K, tbits, (uint64_t)(uintptr_t)e->p.xv,
+          (uint64_t)(uintptr_t)e->p.C, (uint64_t)(uintptr_t)e->p.F, (uint64_t)(uintptr_t)e->p.Jp,
+          (uint64_t)(uintptr_t)e->p.mat, (uint64_t)(uintptr_t)G->ck, (uint64_t)(uintptr_t)G->seg[0],
+          (uint64_t)(uintptr_t)G->seg[1], (uint64_t)(uintptr_t)G->dLdp, (uint64_t)(uintptr_t)e->d_stats};
+}
+
+static cudaError_t grad_begin(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
+                              const double* inv_n) {
+  cudaError_t err = grad_alloc(e, steps, K);
+  if (err != cudaSuccess) return err;
+  JfGrad* G = e->grad;
+  if ((err = cudaMemcpyAsync(G->body_mode, body_mode, sizeof(int32_t) * e->M, cudaMemcpyHostToDevice, e->stream)))
+    return err;
+  if ((err = cudaMemcpyAsync(G->inv_n, inv_n, sizeof(double) * e->M, cudaMemcpyHostToDevice, e->stream)))
+    return err;
+  G->steps = steps;
+  G->K = K;
+  G->t0 = e->t;
+  return cudaSuccess;
+}
+
+static void grad_advance_time(jf_engine* e) {
+  const float dtf = (float)e->dt;
+  float t = e->grad->t0;
+  for (int64_t s = 0; s < e->grad->steps; ++s) t = t + dtf;
+  e->t = t;
+}
+
+cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
+                                 const double* inv_n) {
+  cudaError_t err = grad_begin(e, steps, K, body_mode, inv_n);
+  if (err != cudaSuccess) return err;
+  if ((err = run_graph(e, e->grad->fwd_graph, graph_key(e, 1), [&] { return fwd_record(e); }))) return err;
+  grad_advance_time(e);
+  e->grad->have_forward = true;
+  return cudaSuccess;
+}
+
+cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
+  cudaError_t err = run_graph(e, e->grad->bwd_graph, graph_key(e, 2), [&] { return bwd_record(e); });
+  if (err != cudaSuccess) return err;
+  return bwd_finish(e, gparam_host);
+}
+
+// Forward and backward of one rollout as one graph; the final state's CoM
+// sums are left in e->d_stats for the loss.
+cudaError_t jf_grad_step_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
+                              const double* inv_n, double* gparam_host) {
+  cudaError_t err = grad_begin(e, steps, K, body_mode, inv_n);
+  if (err != cudaSuccess) return err;
+  err = run_graph(e, e->grad->step_graph, graph_key(e, 3), [&] {
+    cudaError_t r = fwd_record(e);
+    if (r == cudaSuccess) r = jf_stats_launch(e);
+    if (r == cudaSuccess) r = bwd_record(e);
+    return r;
+  });
+  if (err != cudaSuccess) return err;
+  grad_advance_time(e);
+  e->grad->have_forward = true;
+  return bwd_finish(e, gparam_host);
 }
 
 // Position adjoint of the initial state for one instance, in engine order.

@@ -246,6 +246,15 @@ class Engine:
                                                    _ptr(g["freq"])))
         return g
 
+    def grad_step(self, steps: int, checkpoint_every: int = 100):
+        """grad_forward + grad_backward as one CUDA graph (replayed on later
+        calls with the same sizes and start time); returns (loss, gradients)."""
+        loss = np.zeros(self.M, np.float64)
+        g = {k: np.zeros(self.M, np.float64) for k in ("actuation", "contraction", "freq")}
+        self._check_run(self._lib.jf_grad_step(self._h, int(steps), int(checkpoint_every), _ptr(loss),
+                                               _ptr(g["actuation"]), _ptr(g["contraction"]), _ptr(g["freq"])))
+        return loss, g
+
     def grad_positions(self, m: int) -> np.ndarray:
         """d loss / d initial positions of instance m, (n_slots, 2) in slot order."""
         out = np.zeros((self.instances[m].n_slots, 2), np.float32)

@@ -233,3 +233,41 @@ def test_gradient_path_reports_nonfinite_states():
     assert rc == L.JF_ERR_NONFINITE
     assert np.isfinite(loss[0])
     e.close()
+
+
+def test_grad_step_graph_matches_forward_and_backward():
+    """jf_grad_step (forward + backward as one CUDA graph, replayed on later
+    calls) against jf_grad_forward + jf_grad_backward and against the same
+    step with graphs off: the deterministic forward gives the same loss bit
+    for bit; the adjoint's float-atomic order moves gradients by ~1e-7."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    pos, mat, fib, prm = grad_cases.small_tank(seed=9)
+    out = {}
+    for name, graphs in (("graph", True), ("direct", False)):
+        e = Engine([InstanceSpec(len(mat), 32, 32, 1.0)] * 2, path="plain", graphs=graphs)
+        e.set_params(**{k: [v, v] for k, v in prm.items()})
+        runs = []
+        for _ in range(3):  # capture, then two replays
+            for m in range(2):
+                e.load(m, pos, mat, fib)
+            e.time = T0
+            loss, g = e.grad_step(STEPS, 15)
+            runs.append((loss, g, e.grad_positions(0), e.time))
+        if graphs:
+            for m in range(2):
+                e.load(m, pos, mat, fib)
+            e.time = T0
+            loss2 = e.grad_forward(STEPS, 15)
+            g2 = e.grad_backward()
+            runs.append((loss2, g2, e.grad_positions(0), e.time))
+        assert not e.error_flags().any()
+        e.close()
+        out[name] = runs
+    ref = out["direct"][0]
+    for loss, g, gx, t in out["graph"] + out["direct"][1:]:
+        assert np.array_equal(loss, ref[0])
+        assert t == ref[3]
+        for k in ("actuation", "contraction", "freq"):
+            np.testing.assert_allclose(g[k], ref[1][k], rtol=1e-5)
+        diff = np.abs(gx - ref[2])
+        assert np.median(diff) <= 1e-6 * np.abs(ref[2]).max()

@@ -65,6 +65,10 @@ def parse():
                     help="substeps of the differentiable rollout leg (checkpoint every 100)")
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiable leg (8 of the workload's instances) and print it")
+    ap.add_argument("--tank-only", action="store_true",
+                    help="run only the tank-loading leg (host fill vs the GPU water fill) and print it")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="run only the plain per-instance path (50 substeps from the loaded inputs) and print it")
     return ap.parse_args()
 
 
@@ -151,12 +155,22 @@ def peaks():
 
 
 def traffic_per_particle_step():
+    """DRAM bytes per live particle-substep of the chunk kernel from the
+    committed ncu measurement, or None when the kernel's sources changed since
+    that measurement (the file records a hash of them)."""
+    import hashlib
     p = os.path.join(HERE, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            d = json.load(f)
-        return d.get("chunk_kernel_dram_bytes_per_live_particle_substep")
-    return None
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    h = hashlib.sha256()
+    for src in d.get("kernel_sources", []):
+        with open(os.path.join(HERE, src), "rb") as f:
+            h.update(f.read())
+    if h.hexdigest()[:16] != d.get("kernel_sources_sha256_16"):
+        return None
+    return d.get("chunk_kernel_dram_bytes_per_live_particle_substep")
 
 
 def cpu_baseline(inputs, target_s=12.0):
@@ -732,6 +746,41 @@ def run_render_only(args):
     return 0
 
 
+def run_tank_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    from jellyfih_b200 import Engine, InstanceSpec
+    engine = Engine([InstanceSpec(args.slots)] * args.instances, path="batched", device=0)
+    out = {"tank": tank_leg(engine, args.instances)}
+    engine.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_plain_only(args, P=50):
+    import torch
+    torch.cuda.set_device(0)
+    from jellyfih_b200 import Engine, InstanceSpec
+    inputs = make_inputs(args.instances, args.slots, 1000)
+    live = sum(int((i[1] >= 0).sum()) for i in inputs)
+    stream = torch.cuda.Stream()
+    plain = Engine([InstanceSpec(args.slots)] * args.instances, path="plain", device=0)
+    plain.set_stream(stream)
+    load_all(plain, inputs)
+    plain.step(5)
+    plain.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    plain.step(P)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    plain.close()
+    print(json.dumps({"plain": {"value": live * P / (ms / 1e3), "unit": UNIT, "substeps": P,
+                                "ms_per_substep": ms / P, "state": "from the loaded inputs"}}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -745,6 +794,10 @@ def main():
         return run_grad_only(args)
     if args.render_only:
         return run_render_only(args)
+    if args.tank_only:
+        return run_tank_only(args)
+    if args.plain_only:
+        return run_plain_only(args)
     return run_ours(args)
 
 

@@ -770,7 +770,16 @@ static cudaError_t grad_alloc(jf_engine* e, int64_t steps, int32_t K) {
     if ((err = alloc_n(&G->dLdp, (size_t)steps * e->M)) != cudaSuccess) return err;
     G->dLdp_cap = (size_t)steps * e->M;
   }
-  // the segment buffers of the backward (K pre-step states and grids, two sets)
+  return cudaSuccess;
+}
+
+// The backward's segment buffers (K pre-step states and grids, two sets),
+// allocated only when a backward runs, so that a forward-only rollout with a
+// long checkpoint interval does not hold them.
+static cudaError_t seg_alloc(jf_engine* e, int32_t K) {
+  JfGrad* G = e->grad;
+  const size_t slots = (size_t)e->total_slots;
+  cudaError_t err = cudaSuccess;
   if (G->seg_cap < (size_t)K) {
     G->seg_cap = 0;
     for (int b = 0; b < 2; ++b) {
@@ -1058,7 +1067,9 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
 }
 
 cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {
-  cudaError_t err = run_graph(e, e->grad->bwd_graph, graph_key(e, 2), [&] { return bwd_record(e); });
+  cudaError_t err = seg_alloc(e, e->grad->K);
+  if (err != cudaSuccess) return err;
+  err = run_graph(e, e->grad->bwd_graph, graph_key(e, 2), [&] { return bwd_record(e); });
   if (err != cudaSuccess) return err;
   return bwd_finish(e, gparam_host);
 }
@@ -1069,6 +1080,7 @@ cudaError_t jf_grad_step_impl(jf_engine* e, int64_t steps, int32_t K, const int3
                               const double* inv_n, double* gparam_host) {
   cudaError_t err = grad_begin(e, steps, K, body_mode, inv_n);
   if (err != cudaSuccess) return err;
+  if ((err = seg_alloc(e, K)) != cudaSuccess) return err;
   err = run_graph(e, e->grad->step_graph, graph_key(e, 3), [&] {
     cudaError_t r = fwd_record(e);
     if (r == cudaSuccess) r = jf_stats_launch(e);

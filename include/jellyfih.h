@@ -42,6 +42,11 @@ extern "C" {
 #define JF_FLAG_AXISYM 4u     /* axisymmetric (r, z) substep, JELLY_AXISYM=1 (mpm_sim.py:17,163-165,
                                  235-268,292-303): r-weighted P2G, hoop-stress correction, v_r = 0
                                  on the axis; the differentiable rollout does not support it */
+#define JF_FLAG_GRAD_FP64 8u  /* the differentiable rollout (jf_grad_*) in FP64: the same kernels
+                                 built for double, every constant the reference's Python double,
+                                 P2G summed with double atomics; the state is widened from the
+                                 engine's FP32 particles and the final state written back rounded
+                                 to FP32.  Stepping (jf_step etc.) stays FP32 */
 
 typedef struct jf_engine jf_engine;
 

@@ -21,6 +21,7 @@ JF_PATH_BATCHED = 1
 JF_FLAG_GLOW = 1
 JF_FLAG_NO_GRAPHS = 2
 JF_FLAG_AXISYM = 4
+JF_FLAG_GRAD_FP64 = 8
 JF_VORT_RDBU = 0
 JF_VORT_HUESHIFT = 1
 JF_VORT_WHITE = 2

@@ -17,7 +17,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libjellyfih.so")
 SOURCES = ["jf_capi.cu", "jf_plain.cu", "jf_batched.cu", "jf_noalloc.cu", "jf_grad.cu", "jf_render.cu", "jf_tank.cu"]
-HEADERS = ["jf_device.cuh", "jf_engine.h", "jf_dual.cuh"]
+HEADERS = ["jf_device.cuh", "jf_device64.cuh", "jf_engine.h", "jf_dual.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

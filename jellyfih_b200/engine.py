@@ -45,12 +45,14 @@ class Engine:
     instance and substep, as the reference's substep() offloads do.
     ``axisym=True`` runs the axisymmetric (r, z) substep of JELLY_AXISYM=1
     (every instance; the load positions' x becomes each particle's r_ref).
+    ``grad_fp64=True`` runs the differentiable rollout (grad_forward /
+    grad_backward / grad_step) in FP64, the same kernels built for double.
     """
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
                  block_threads: int = 512, cluster_size: int = 0, graphs: bool = True,
-                 cell_cap: int = 0, axisym: bool = False):
+                 cell_cap: int = 0, axisym: bool = False, grad_fp64: bool = False):
         self._lib = L.load()
         self.instances = list(instances)
         self.M = len(self.instances)
@@ -58,7 +60,7 @@ class Engine:
         descs = (L.JfInstanceDesc * self.M)(*[
             L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
         flags = ((L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
-                 | (L.JF_FLAG_AXISYM if axisym else 0))
+                 | (L.JF_FLAG_AXISYM if axisym else 0) | (L.JF_FLAG_GRAD_FP64 if grad_fp64 else 0))
         cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
                          flags, device, resort_interval, block_threads, cluster_size, cell_cap)
         h = L._E()

@@ -5,7 +5,7 @@ central differences of the oracle, for the FP32 kernels and their FP64 build.
 checkpoint every 100.  The CUDA gradient of the payload CoM displacement with
 respect to the actuation amplitude, the contraction fraction (the refractory
 fraction is 1 - contraction: its gradient is the negative), the frequency
-multiplier and 8 seeded particles' initial positions is compared with central
+multiplier and 64 seeded particles' initial positions is compared with central
 differences of the FP64 build of the oracle, run as one OpenMP batch of all
 perturbed copies: the genes at the configuration's step (1e-3, and 1e-3 of
 the amplitude) and at 1e-5 (1e-5 of the amplitude), positions at 1e-5 dx.
@@ -16,7 +16,8 @@ What was measured (one B200):
 * The FP64 build of the kernels is the derivative of the discrete rollout:
   against the 1e-5 differences its gene gradients agree within 2e-7 to 3e-5
   relative (medians 1.1e-5 actuation, 1.5e-5 contraction, 8e-6 frequency),
-  its position gradients within 2.4e-6 of the gradient's max-norm, its loss
+  its position gradients within 1.9e-5 of the gradient's max-norm (median
+  6.5e-7), its loss
   within 2e-7 to 4e-5 of the FP64 oracle's (3e-4 for instance 7).  Two
   exceptions are the differences' own: the contraction of instances 3 and 4
   is not linear even at 1e-5 (the 1e-3 and 1e-5 differences of instance 3
@@ -32,9 +33,9 @@ What was measured (one B200):
   over 2,000 substeps (near-incompressible water amplifies rounding ~1e3 per
   substep; one instance ends 109 % off in displacement), so their gradients
   agree with FP64 differences within 0.3-3 % on the instances whose FP32
-  trajectory tracks FP64 and are off by more than 100 % on others; water
-  particles' position gradients within 4e-3 of the max-norm, payload
-  particles' up to 0.47.
+  trajectory tracks FP64 and are off by more than 100 % on others; position
+  gradients of water particles within 1.9e-2 of the max-norm (median 3e-5),
+  of jelly and muscle within 6.4e-3, of payload up to 0.29.
 * The waveform drop (instance 7): the 1e-3 differences spread the drop over
   +-25 substeps; the CUDA gradient of the contraction, carried by the drop's
   boundary term, is within 10 % of them in both precisions.
@@ -116,8 +117,9 @@ def test_config4_gradients_against_fp64_differences():
     pos, mat, fib = inputs[m_pos][:3]
     rng = np.random.default_rng(4)
     live = np.flatnonzero(mat >= 0)
-    pick = np.concatenate([rng.choice(np.flatnonzero(mat == 2), 4, replace=False),
-                           rng.choice(np.flatnonzero(mat == 0), 4, replace=False)])
+    # 64 seeded particles: 8 of each robot material (jelly, payload, muscle), the rest water
+    robot = [rng.choice(np.flatnonzero(mat == k), 8, replace=False) for k in (1, 2, 3)]
+    pick = np.concatenate(robot + [rng.choice(np.flatnonzero(mat == 0), 64 - 24, replace=False)])
     hx = 1e-5 / 128
     for k in pick:
         for a in (0, 1):
@@ -188,4 +190,5 @@ def test_config4_gradients_against_fp64_differences():
         assert np.all(np.isfinite(err[("fp32", name, 1)]))
         assert np.median(err[("fp32", name, 0)]) <= 0.5, (name, err[("fp32", name, 0)])
     water = [i for i, k in enumerate(np.repeat(pick, 2)) if mat[k] == 0]
-    assert pos_err["fp32"][water].max() <= 2e-2, pos_err["fp32"]
+    assert np.median(pos_err["fp32"][water]) <= 1e-3, pos_err["fp32"]
+    assert pos_err["fp32"][water].max() <= 5e-2, pos_err["fp32"]

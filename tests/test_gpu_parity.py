@@ -162,6 +162,75 @@ def _oracle_run(pos, mat, fib, c, f, steps, nx=128, ny=128, dh=1.0, act=500.0, p
 
 
 
+def _small_cluster(n_slots):
+    """A few particles of every material around (0.5, 0.5) at the lattice
+    spacing dx/2, dead slots interleaved."""
+    dx = 1.0 / 128
+    pos = np.full((n_slots, 2), -1.0, np.float32)
+    mat = np.full(n_slots, -1, np.int32)
+    fib = np.zeros((n_slots, 2), np.float32)
+    fib[:, 1] = 1.0
+    k = 0
+    for j in range(5):
+        for i in range(5):
+            if k >= n_slots - 1:
+                break
+            pos[k] = (0.5 + 0.5 * dx * i, 0.5 + 0.5 * dx * j)
+            mat[k] = (1, 3, 2, 0)[(i + 2 * j) % 4]
+            fib[k] = (0.6, 0.8) if mat[k] == 3 else (0.0, 1.0)
+            k += 2 if (i + j) % 3 == 0 else 1  # leave some slots dead
+    return pos, mat, fib
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_degenerate_instances_match_oracle(path):
+    """Instances with nothing to step beside a full tank: all slots dead,
+    water only (no payload and no body: zero CoM rows, as the reference
+    returns for count 0), one payload particle in one slot, zero slots, and a
+    ragged 37-slot cluster of every material; 64 substeps, rows and states
+    against the oracle."""
+    from jellyfih_b200 import InstanceSpec
+    from oracle import oracle as O
+    pos0, mat0, fib0, st, c, f = _tank_instance(41)
+    dead = (np.full((80000, 2), -1.0, np.float32), np.full(80000, -1, np.int32),
+            np.zeros((80000, 2), np.float32))
+    water_mat = np.where(mat0 > 0, -1, mat0).astype(np.int32)
+    one = (np.array([[0.5, 0.6]], np.float32), np.array([2], np.int32), np.array([[0.0, 1.0]], np.float32))
+    empty = (np.zeros((0, 2), np.float32), np.zeros(0, np.int32), np.zeros((0, 2), np.float32))
+    cases = [(pos0, mat0, fib0), dead, (pos0, water_mat, fib0), one, empty, _small_cluster(37)]
+    e = _engine([InstanceSpec(len(m)) for _, m, _ in cases], path)
+    for m, (p, mt, fb) in enumerate(cases):
+        if len(mt):
+            e.load(m, p, mt, fb)
+    e.set_params(contraction=[c] * len(cases), freq=[f] * len(cases))
+    res = e.run_headless(64)
+    assert not e.error_flags().any()
+    stats = e.stats_any()
+    for m, (p, mt, fb) in enumerate(cases):
+        s, ref = _oracle_run(p, mt, fb, c, f, 64)
+        np.testing.assert_allclose(res[m], ref, rtol=1e-6, atol=1e-7, err_msg=f"inst{m} rows")
+        ref_stats = O.stats_any([s["x"]], [s["material"]])[0]
+        np.testing.assert_allclose(stats[m], ref_stats, rtol=1e-6, atol=1e-7, err_msg=f"inst{m} stats")
+        if not len(mt):
+            continue
+        got = e.read(m)
+        live = mt >= 0
+        assert np.array_equal(got["x"][~live], p[~live]), m  # dead slots are not touched
+        if not live.any():
+            continue
+        if m in (0, 2):  # full tanks: the water's order noise, bounds of the uneven-batch test
+            assert np.abs(got["x"][live] - s["x"][live]).max() < 2e-5, m
+            assert_norm_close(got["v"][live], s["v"][live], 2e-2, f"inst{m} v")
+            assert_norm_close(got["F"][live], s["F"][live], 1e-4, f"inst{m} F")
+            continue
+        assert np.abs(got["x"][live] - s["x"][live]).max() < 1e-6, m
+        for k in ("v", "C", "F"):
+            assert_norm_close(got[k][live], s[k][live], 1e-5, f"inst{m} {k}")
+    for m in (1, 2, 4):
+        assert not res[m].any() and not stats[m].any()
+    e.close()
+
+
 def test_batched_odd_grids_against_oracle():
     """Grid widths that are not multiples of 32 and do not divide the block
     (80 x 112 and 96 x 96 nodes): partial 32-cell segments, the generic grid

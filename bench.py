@@ -341,9 +341,26 @@ def grad_leg(inputs, device, stream, steps=2000, checkpoint_every=100):
     fast = ev[0].elapsed_time(ev[1])
     b.close()
     e.close()
+    # the FP64 build of the same kernels on the same rollout
+    d = Engine([InstanceSpec(len(inputs[0][1]))] * M, path="plain", device=device, grad_fp64=True)
+    d.set_stream(stream)
+    times = []
+    for _ in range(2):  # the first pass loads the FP64 kernels and allocates their buffers
+        load_all(d, inputs)
+        d.time = 0.0
+        ev[0].record(stream)
+        d.grad_forward(steps, checkpoint_every)
+        ev[1].record(stream)
+        d.grad_backward()
+        ev[2].record(stream)
+        ev[2].synchronize()
+        times.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
+    d.close()
+    fwd64, bwd64 = times[-1]
     return {"instances": M, "substeps": steps, "checkpoint_every": checkpoint_every,
             "fwd_ms": fwd, "bwd_ms": bwd, "fwd_bwd_over_fwd": (fwd + bwd) / fwd,
-            "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast}
+            "batched_fwd_ms": fast, "fwd_bwd_over_batched_fwd": (fwd + bwd) / fast,
+            "fp64": {"fwd_ms": fwd64, "bwd_ms": bwd64, "fwd_bwd_over_fwd": (fwd64 + bwd64) / fwd64}}
 
 
 def plain_leg(inputs, spec, device, stream, S, W, K, batched_value, live, points=4, P=50):

@@ -1275,16 +1275,22 @@ cudaError_t run_graph(jf_engine* e, GradGraph& gg, const std::vector<uint64_t>& 
   return cudaGraphLaunch(gg.exec, e->stream);
 }
 
+// What a captured graph depends on.  The forward (tag 1) does not touch the
+// segment buffers, which the first backward allocates: they stay out of its
+// key, so that a forward captured before any backward is still replayed.
 template <class R>
 std::vector<uint64_t> graph_key(jf_engine* e, int tag) {
   const GradBuffers<R>& G = bufs<R>(e);
   uint64_t tbits = 0;
   memcpy(&tbits, &G.t0, sizeof(R));
+  const bool segs = tag != 1;
   return {(uint64_t)tag, (uint64_t)sizeof(R), (uint64_t)G.steps, (uint64_t)G.K, tbits,
           (uint64_t)(uintptr_t)e->p.xv, (uint64_t)(uintptr_t)e->p.C, (uint64_t)(uintptr_t)e->p.F,
           (uint64_t)(uintptr_t)e->p.Jp, (uint64_t)(uintptr_t)e->p.mat, (uint64_t)(uintptr_t)G.ck,
-          (uint64_t)(uintptr_t)G.seg[0], (uint64_t)(uintptr_t)G.seg[1], (uint64_t)(uintptr_t)G.dLdp,
-          (uint64_t)(uintptr_t)e->d_stats};
+          segs ? (uint64_t)(uintptr_t)G.seg[0] : 0, segs ? (uint64_t)(uintptr_t)G.seg[1] : 0,
+          segs ? (uint64_t)(uintptr_t)G.useg[0] : 0, segs ? (uint64_t)(uintptr_t)G.useg[1] : 0,
+          segs ? (uint64_t)(uintptr_t)G.pmseg[0] : 0, segs ? (uint64_t)(uintptr_t)G.pmseg[1] : 0,
+          (uint64_t)(uintptr_t)G.dLdp, (uint64_t)(uintptr_t)e->d_stats};
 }
 
 template <class R>

@@ -224,8 +224,12 @@ def test_degenerate_instances_match_oracle(path):
             assert_norm_close(got["F"][live], s["F"][live], 1e-4, f"inst{m} F")
             continue
         assert np.abs(got["x"][live] - s["x"][live]).max() < 1e-6, m
-        for k in ("v", "C", "F"):
+        for k in ("v", "F"):
             assert_norm_close(got[k][live], s[k][live], 1e-5, f"inst{m} {k}")
+        # C is a velocity difference over dx: for a lone particle in a uniform
+        # field it is rounding noise (~1e-7), so its scale is max|v| / dx
+        c_scale = np.abs(s["v"][live]).max() * 128
+        assert np.abs(got["C"][live] - s["C"][live]).max() <= 1e-5 * c_scale, m
     for m in (1, 2, 4):
         assert not res[m].any() and not stats[m].any()
     e.close()

@@ -33,6 +33,8 @@ extern "C" {
                                  also flags P2G contributions too large for its fixed-point sums
                                  and non-finite adjoint states */
 #define JF_ERR_UNSUPPORTED 4  /* configuration outside what the chosen path supports */
+#define JF_ERR_TIMEOUT 5      /* jf_sync_timeout: the engine's queued work had not finished
+                                 within the limit; it keeps running, the engine stays usable */
 
 #define JF_PATH_PLAIN 0       /* one instance per launch sequence (reference structure) */
 #define JF_PATH_BATCHED 1     /* all instances in one persistent cluster launch per chunk */
@@ -111,6 +113,14 @@ int jf_get_time(const jf_engine* e, float* t);
 /* n substeps of every instance (n calls of substep(), mpm_sim.py:153-340). */
 int jf_step(jf_engine* e, int64_t n_steps);
 int jf_sync(jf_engine* e);
+
+/* jf_sync with a watchdog limit: waits at most timeout_ms milliseconds for
+ * the work queued on the engine's stream (jf_step returns once its launches
+ * are queued; ti.sync(), run_population.py:37,47,73, is the reference's
+ * unbounded wait).  JF_ERR_TIMEOUT if it has not finished by then: nothing is
+ * cancelled, the work runs on, and a later jf_sync or jf_sync_timeout waits
+ * for it.  Otherwise the same as jf_sync. */
+int jf_sync_timeout(jf_engine* e, int64_t timeout_ms);
 
 /* get_payload_stats (mpm_sim.py:764-777): out[n_instances][3] =
  * [com_y, com_x, count] of the payload (material 2), zeros without payload.

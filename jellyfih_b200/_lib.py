@@ -16,6 +16,7 @@ JF_ERR_INVALID = 1
 JF_ERR_CUDA = 2
 JF_ERR_NONFINITE = 3
 JF_ERR_UNSUPPORTED = 4
+JF_ERR_TIMEOUT = 5
 JF_PATH_PLAIN = 0
 JF_PATH_BATCHED = 1
 JF_FLAG_GLOW = 1
@@ -57,6 +58,7 @@ EXPORTS = {
     "jf_get_time": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_float)]),
     "jf_step": (ctypes.c_int, [_E, ctypes.c_int64]),
     "jf_sync": (ctypes.c_int, [_E]),
+    "jf_sync_timeout": (ctypes.c_int, [_E, ctypes.c_int64]),
     "jf_payload_stats": (ctypes.c_int, [_E, _P]),
     "jf_stats_any": (ctypes.c_int, [_E, _P]),
     "jf_stats_raw": (ctypes.c_int, [_E, _P]),

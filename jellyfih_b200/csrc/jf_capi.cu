@@ -4,7 +4,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -626,6 +628,25 @@ int jf_sync(jf_engine* e) {
   std::vector<int32_t> flags;
   if ((rc = read_flags_and_sync(e, flags))) return rc;
   return nonfinite_status(e, flags);
+}
+
+int jf_sync_timeout(jf_engine* e, int64_t timeout_ms) {
+  if (check_engine(e)) return JF_ERR_INVALID;
+  if (timeout_ms < 0) return fail(e, JF_ERR_INVALID, "jf_sync_timeout: negative limit");
+  int rc = set_device(e);
+  if (rc) return rc;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t q = cudaStreamQuery(e->stream);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) return cuda_fail(e, q, "stream query");
+    const auto waited = std::chrono::duration_cast<std::chrono::milliseconds>(
+        std::chrono::steady_clock::now() - t0).count();
+    if (waited >= timeout_ms)
+      return fail(e, JF_ERR_TIMEOUT, "queued work not finished after " + std::to_string(waited) + " ms");
+    std::this_thread::sleep_for(std::chrono::microseconds(100));
+  }
+  return jf_sync(e);
 }
 
 int jf_payload_stats(jf_engine* e, double* out) {

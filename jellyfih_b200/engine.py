@@ -168,8 +168,18 @@ class Engine:
     def step(self, n: int = 1) -> None:
         self._check(self._lib.jf_step(self._h, int(n)))
 
-    def sync(self) -> None:
-        self._check_run(self._lib.jf_sync(self._h))
+    def sync(self, timeout: float | None = None) -> bool:
+        """Waits for the queued work (ti.sync()).  With a timeout in seconds,
+        waits at most that long and returns False if the work is still
+        running (it is not cancelled; a later sync waits for it)."""
+        if timeout is None:
+            self._check_run(self._lib.jf_sync(self._h))
+            return True
+        rc = self._lib.jf_sync_timeout(self._h, int(max(timeout, 0.0) * 1000))
+        if rc == L.JF_ERR_TIMEOUT:
+            return False
+        self._check_run(rc)
+        return True
 
     # -- readback ------------------------------------------------------------
     def payload_stats(self) -> np.ndarray:

@@ -57,6 +57,7 @@ def test_create_rejects_bad_config_before_touching_the_device(lib):
 def test_null_handle_calls_fail_cleanly(lib):
     assert lib.jf_step(None, 1) == L.JF_ERR_INVALID
     assert lib.jf_sync(None) == L.JF_ERR_INVALID
+    assert lib.jf_sync_timeout(None, 10) == L.JF_ERR_INVALID
     assert lib.jf_payload_stats(None, None) == L.JF_ERR_INVALID
     assert lib.jf_destroy(None) == L.JF_ERR_INVALID
     assert lib.jf_kernel_launches(None) == -1

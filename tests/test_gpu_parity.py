@@ -395,6 +395,39 @@ def test_nonfinite_flag_and_invalid_arguments():
     e.close()
 
 
+def test_sync_timeout_reports_unfinished_work_and_recovers():
+    """The watchdog wait: jf_sync_timeout returns JF_ERR_TIMEOUT while queued
+    substeps still run, cancels nothing, and a later wait collects them with
+    the work complete: the same time and live, finite particles as a run
+    waited for without a limit."""
+    from jellyfih_b200 import InstanceSpec
+    from jellyfih_b200 import _lib as L
+    pos, mat, fib, st, c, f = _tank_instance(51, n_slots=20000, grid=64, ny=64)
+    steps = 20000  # ~0.4 s of chunks, queued in ~1 ms
+    runs = []
+    for limited in (True, False):
+        e = _engine([InstanceSpec(20000, 64, 64)] * 4, "batched")
+        for m in range(4):
+            e.load(m, pos, mat, fib)
+        e.set_params(contraction=[c] * 4, freq=[f] * 4)
+        e.sync()
+        e.step(steps)
+        if limited:
+            assert e._lib.jf_sync_timeout(e._h, 0) == L.JF_ERR_TIMEOUT
+            assert b"not finished" in e._lib.jf_last_error(e._h)
+            assert e._lib.jf_sync_timeout(e._h, -1) == L.JF_ERR_INVALID
+            assert e.sync(timeout=120.0) is True
+        else:
+            e.sync()
+        assert not e.error_flags().any()
+        runs.append((e.time, e.read(3)["x"]))
+        e.close()
+    live = mat >= 0
+    assert runs[0][0] == runs[1][0]
+    for _, x in runs:
+        assert np.isfinite(x[live]).all() and (x[live] > 0).all() and (x[live] < 1).all()
+
+
 def test_mpm_sim_module_drop_in(monkeypatch):
     """The drop-in module runs the reference's evolve.py-style call sequence."""
     import importlib

@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
 
   for (int n = tid; n < n_planes * WN; n += nth) sm[n] = 0.0f;
   unsigned n_fast = 0, n_generic = 0, n_gather_generic = 0, n_overflow = 0;
+  bool nonfinite = false;  // a G2P result of this thread's particles was NaN/Inf
   cluster.sync();
 
   // G2P of the previous substep, then P2G of this one, for a particle that
@@ -323,7 +324,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     if (do_g2p) {
       jf_g2p_particle(I, x, v, C, [&](int ni, int nj) { return gather_node(w, cluster, ni, nj); });
       if (a.do_glow) a.glow[g] = jf_glow(a.glow[g], jp);
-      if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
+      nonfinite |= !(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y));
       a.xv[g] = make_float4(x.x, x.y, v.x, v.y);
       if (!do_p2g) a.C[g] = C;  // stored when no later pass of the chunk recomputes it (see the cell loop)
     }
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
           }
           jf_g2p_advect(I, x, v);
           if (a.do_glow) a.glow[p0 + k] = jf_glow(a.glow[p0 + k], jp);
-          if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) atomicOr(a.err + m, 1);
+          nonfinite |= !(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y));
           xv_m[k] = make_float4(x.x, x.y, v.x, v.y);
           // this pass's P2G takes C from registers and the next pass's G2P
           // recomputes it, so C is stored only by the chunk's last pass and
@@ -571,6 +572,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
       __syncthreads();
     }
   }
+  if (__any_sync(0xffffffffu, nonfinite) && lane == 0) atomicOr(a.err + m, 1);
   // path counters: one atomic per warp
   if (a.path) {
     const unsigned f = __reduce_add_sync(0xffffffffu, n_fast);

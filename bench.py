@@ -69,6 +69,12 @@ def parse():
                     help="run only the tank-loading leg (host fill vs the GPU water fill) and print it")
     ap.add_argument("--plain-only", action="store_true",
                     help="run only the plain per-instance path (50 substeps from the loaded inputs) and print it")
+    ap.add_argument("--grad-checkpoint", type=int, default=100,
+                    help="checkpoint interval of the differentiable rollout leg")
+    ap.add_argument("--episode-only", action="store_true",
+                    help="run only the end-to-end episode leg (jf_run_episode, --steps episodes of --substeps)")
+    ap.add_argument("--noalloc-only", action="store_true",
+                    help="run only the allocation-free substep (jf_substep_noalloc) on one instance, --substeps calls")
     return ap.parse_args()
 
 
@@ -692,7 +698,8 @@ def run_ours(args):
         # points inside the window of substeps the batched value averages over
         extras["plain"] = plain_leg(inputs, spec, local, stream, S, W, K, value, live)
 
-        extras["differentiable"] = grad_leg(inputs[:8], local, stream, steps=args.grad_substeps)
+        extras["differentiable"] = grad_leg(inputs[:8], local, stream, steps=args.grad_substeps,
+                                            checkpoint_every=args.grad_checkpoint)
         if not args.no_refine:
             extras["refine"] = refine_leg(local, stream)
 
@@ -739,7 +746,8 @@ def run_grad_only(args):
     torch.cuda.set_device(0)
     inputs = make_inputs(args.instances, args.slots, 1000)
     stream = torch.cuda.Stream()
-    out = {"differentiable": grad_leg(inputs[:8], 0, stream, steps=args.grad_substeps)}
+    out = {"differentiable": grad_leg(inputs[:8], 0, stream, steps=args.grad_substeps,
+                                      checkpoint_every=args.grad_checkpoint)}
     if not args.no_refine:
         out["refine"] = refine_leg(0, stream)
     print(json.dumps(out), flush=True)
@@ -798,6 +806,84 @@ def run_plain_only(args, P=50):
     return 0
 
 
+def run_episode_only(args):
+    """jf_run_episode alone: every instance loaded from pinned host arrays, a
+    headless run of --substeps, GPU fitness, rows and fitness read back."""
+    import torch
+    torch.cuda.set_device(0)
+    from jellyfih_b200 import Engine, InstanceSpec
+    inputs = make_inputs(args.instances, args.slots, 1000)
+    live = sum(int((i[1] >= 0).sum()) for i in inputs)
+    engine = Engine([InstanceSpec(args.slots)] * args.instances, path="batched", device=0)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    pos_all = pin(np.concatenate([i[0] for i in inputs]))
+    mat_all = pin(np.concatenate([i[1] for i in inputs]))
+    fib_all = pin(np.concatenate([i[2] for i in inputs]))
+    con = np.array([i[3] for i in inputs], np.float32)
+    frq = np.array([i[4] for i in inputs], np.float32)
+    mus = np.array([i[5]["muscle_count"] for i in inputs], np.int32)
+    run = lambda: engine.run_episode(pos_all, mat_all, con, args.substeps, fibers=fib_all, freq=frq,  # noqa: E731
+                                     muscle_counts=mus)
+    run()  # allocates the call's staging buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res, fit = run()
+    el = time.perf_counter() - t0
+    engine.close()
+    print(json.dumps({"episode": {"value": live * args.substeps * args.steps / el, "unit": UNIT,
+                                  "episodes": args.steps, "substeps": args.substeps,
+                                  "valid": int(res[:, 4].sum())}}), flush=True)
+    return 0
+
+
+def run_noalloc_only(args):
+    """jf_substep_noalloc alone: one instance of the workload on caller-owned
+    device arrays (the engine's state after 300 substeps), --substeps calls,
+    CUDA events around them."""
+    import torch
+    torch.cuda.set_device(0)
+    from jellyfih_b200 import Engine, InstanceSpec, _lib
+    pos, mat, fib, c, f, st = make_inputs(1, args.slots, 1000)[0]
+    live = int((mat >= 0).sum())
+    eng = Engine([InstanceSpec(args.slots)], path="plain", device=0)
+    eng.load(0, pos, mat, fib)
+    eng.set_params(contraction=[c], freq=[f])
+    eng.time = 0.0
+    eng.step(300)
+    s0 = eng.read(0)
+    t = eng.time
+    eng.close()
+    dev = torch.device("cuda", 0)
+    fields = ("x", "v", "C", "F", "material", "Jp", "glow", "fiber")
+    bufs = {k: torch.from_numpy(np.ascontiguousarray(s0[k])).to(dev) for k in fields}
+    ptrs = [bufs[k].data_ptr() for k in fields]
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    dt = np.float32(2e-5)
+
+    def call(t):
+        rc = lib.jf_substep_noalloc(args.slots, 128, 128, 1.0, float(dt), float(t), 500.0, float(c), float(f),
+                                    2.5, *ptrs, stream.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(lib.jf_last_error(None).decode())
+        return np.float32(t + dt)
+
+    for _ in range(5):
+        t = call(t)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.substeps):
+        t = call(t)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    print(json.dumps({"noalloc": {"value": live * args.substeps / (ms / 1e3), "unit": UNIT,
+                                  "substeps": args.substeps, "us_per_substep": ms / args.substeps * 1e3,
+                                  "live_particles": live}}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -815,6 +901,10 @@ def main():
         return run_tank_only(args)
     if args.plain_only:
         return run_plain_only(args)
+    if args.episode_only:
+        return run_episode_only(args)
+    if args.noalloc_only:
+        return run_noalloc_only(args)
     return run_ours(args)
 
 

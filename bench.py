@@ -493,7 +493,26 @@ def render_leg(engine, stream, M, cpu, frames=20, res=1024):
     ms = ev[0].elapsed_time(ev[1]) / frames
     abyss_ms = ev[1].elapsed_time(ev[2]) / frames
     live = sum(int((engine.read(m)["material"] >= 0).sum()) for m in range(M))
-    out = {"ms_per_frame": ms, "frames_per_s": 1e3 / ms, "abyss_ms": abyss_ms,
+    # the web viewers' flat frame (payload_sink.py, view_*.py): white clear and
+    # one single-colour splat pass per palette entry (mpm_sim.py WEB_PALETTE)
+    palette = ((0, 0.933, 0.949, 0.957), (1, 0.678, 0.882, 0.875), (3, 0.976, 0.757, 0.765),
+               (2, 0.961, 0.824, 0.576))
+    flat_radius = max(1.0, rs / 128 * 0.6)
+
+    def flat_frame():
+        engine.frame_clear(1.0)
+        for mat_id, r, g, b in palette:
+            engine.render_flat(rs, gs, flat_radius, mat_id, r, g, b)
+
+    for _ in range(3):
+        flat_frame()
+    ev[2].record(stream)
+    for _ in range(frames):
+        flat_frame()
+    ev[3].record(stream)
+    ev[3].synchronize()
+    flat_ms = ev[2].elapsed_time(ev[3]) / frames
+    out = {"ms_per_frame": ms, "frames_per_s": 1e3 / ms, "abyss_ms": abyss_ms, "flat_ms_per_frame": flat_ms,
            "splat_particles_per_s": live / (abyss_ms / 1e3), "video_res": res, "grid_side": gs,
            "res_sub": rs, "particles": live, "kernels_per_frame": launches / frames,
            "pipeline": "clear, abyss (rainbow water, radius 1.5), vorticity overlay, tone map, vorticity grid, rdbu"}
@@ -759,13 +778,15 @@ def run_render_only(args):
     torch.cuda.set_device(0)
     from jellyfih_b200 import Engine, InstanceSpec
     inputs = make_inputs(args.instances, args.slots, 1000)
-    engine = Engine([InstanceSpec(args.slots)] * args.instances, path="batched", device=0)
+    # the viewers step with the render-only glow on (JELLY_B200_GLOW=1)
+    engine = Engine([InstanceSpec(args.slots)] * args.instances, path="batched", device=0, glow=True)
     stream = torch.cuda.Stream()
     engine.set_stream(stream)
     load_all(engine, inputs)
     engine.step(args.substeps)
     engine.sync()
-    out = {"render": render_leg(engine, stream, args.instances, cpu=True), "substeps_before": args.substeps}
+    out = {"render": render_leg(engine, stream, args.instances, cpu=True), "substeps_before": args.substeps,
+           "glow": True}
     engine.close()
     print(json.dumps(out), flush=True)
     return 0

@@ -850,7 +850,7 @@ int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, doubl
   std::vector<double> inv_n, init;
   if ((rc = grad_prologue(e, body, inv_n, init))) return rc;
   JF_CK(jf_grad_forward_impl(e, steps, checkpoint_every, body.data(), inv_n.data()), "gradient forward");
-  JF_CK(jf_stats_launch(e), "stats kernel");
+  JF_CK(jf_grad_loss_stats(e), "loss sums");
   if ((rc = grad_loss(e, body, init, loss))) return rc;
   e->sorted = false;
   std::vector<int32_t> flags;

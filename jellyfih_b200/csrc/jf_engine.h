@@ -154,6 +154,8 @@ cudaError_t jf_grad_step_impl(jf_engine* e, int64_t steps, int32_t K, const int3
                               const double* inv_n, double* gparam_host);
 cudaError_t jf_grad_x0_impl(jf_engine* e, int m, std::vector<float4>& out);
 void jf_grad_free(jf_engine* e);
+// The rollout's loss sums into e->d_stats (from the FP64 final state in the FP64 build).
+cudaError_t jf_grad_loss_stats(jf_engine* e);
 
 // CoM sums of every instance into e->d_stats (M x 6 doubles).
 cudaError_t jf_stats_launch(jf_engine* e);

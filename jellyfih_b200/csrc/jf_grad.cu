@@ -44,6 +44,7 @@
 // build.  In FP64 the P2G sums are plain double atomics (their order moves
 // results by ~1e-16), the working state is a double copy of the engine's
 // particles, and the final state is written back to them rounded to FP32.
+#include <algorithm>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -694,6 +695,41 @@ __global__ void narrow_kernel(const JfInst* __restrict__ inst, JfParticles p, co
   p.Jp[g] = (float)Jp[g];
 }
 
+// The loss sums of the FP64 build from its own final state (the FP32 slots
+// hold it rounded): per instance payload [sum_y, count, sum_x] and body
+// (jelly + muscle) [sum_y, count, sum_x], as stats_kernel sums the FP32 slots.
+__global__ void stats64_kernel(const JfInst* __restrict__ inst, const double4* __restrict__ xv,
+                               const int32_t* __restrict__ mat, double* __restrict__ out) {
+  const int m = blockIdx.y;
+  const JfInst I = inst[m];
+  double py = 0, pc = 0, px = 0, by = 0, bc = 0, bx = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < I.n_slots; k += gridDim.x * blockDim.x) {
+    const int64_t g = I.p_off + k;
+    const int mt = mat[g];
+    if (mt == 2) {
+      const double4 a = xv[g];
+      py += a.y; pc += 1.0; px += a.x;
+    } else if (mt == 1 || mt == 3) {
+      const double4 a = xv[g];
+      by += a.y; bc += 1.0; bx += a.x;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    py += __shfl_down_sync(0xffffffffu, py, off);
+    pc += __shfl_down_sync(0xffffffffu, pc, off);
+    px += __shfl_down_sync(0xffffffffu, px, off);
+    by += __shfl_down_sync(0xffffffffu, by, off);
+    bc += __shfl_down_sync(0xffffffffu, bc, off);
+    bx += __shfl_down_sync(0xffffffffu, bx, off);
+  }
+  if ((threadIdx.x & 31) == 0 && (pc > 0 || bc > 0)) {
+    double* o = out + 6 * m;
+    atomicAdd(o + 0, py); atomicAdd(o + 1, pc); atomicAdd(o + 2, px);
+    atomicAdd(o + 3, by); atomicAdd(o + 4, bc); atomicAdd(o + 5, bx);
+  }
+}
+
 template <class T>
 cudaError_t alloc_n(T** p, size_t n) {
   return cudaMalloc((void**)p, sizeof(T) * (n > 0 ? n : 1));
@@ -1335,6 +1371,24 @@ cudaError_t backward_impl(jf_engine* e, double* gparam_host) {
   return bwd_finish<R>(e, gparam_host);
 }
 
+// The loss sums into e->d_stats after a rollout: the engine's stats over its
+// FP32 slots, or, in the FP64 build, over the FP64 final state.
+template <class R>
+cudaError_t loss_stats(jf_engine* e) {
+  if constexpr (std::is_same<R, double>::value) {
+    GradBuffers<double>& G = bufs<double>(e);
+    cudaError_t err = cudaMemsetAsync(e->d_stats, 0, sizeof(double) * 6 * e->M, e->stream);
+    if (err != cudaSuccess) return err;
+    const int blocks = std::max(1, std::min(64, (int)((e->max_slots + kT - 1) / kT)));
+    stats64_kernel<<<dim3(blocks, e->M), kT, 0, e->stream>>>(e->d_inst, state_at<double>(G.fin, e->total_slots, 0).xv,
+                                                             e->p.mat, e->d_stats);
+    e->launches += 1;
+    return cudaGetLastError();
+  } else {
+    return jf_stats_launch(e);
+  }
+}
+
 template <class R>
 cudaError_t step_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode, const double* inv_n,
                       double* gparam_host) {
@@ -1343,7 +1397,7 @@ cudaError_t step_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* bod
   if ((err = seg_alloc<R>(e, K)) != cudaSuccess) return err;
   err = run_graph(e, bufs<R>(e).step_graph, graph_key<R>(e, 3), [&] {
     cudaError_t r = fwd_record<R>(e);
-    if (r == cudaSuccess) r = jf_stats_launch(e);
+    if (r == cudaSuccess) r = loss_stats<R>(e);
     if (r == cudaSuccess) r = bwd_record<R>(e);
     return r;
   });
@@ -1376,6 +1430,10 @@ cudaError_t jf_grad_forward_impl(jf_engine* e, int64_t steps, int32_t K, const i
                                  const double* inv_n) {
   return fp64(e) ? forward_impl<double>(e, steps, K, body_mode, inv_n)
                  : forward_impl<float>(e, steps, K, body_mode, inv_n);
+}
+
+cudaError_t jf_grad_loss_stats(jf_engine* e) {
+  return fp64(e) ? loss_stats<double>(e) : loss_stats<float>(e);
 }
 
 cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host) {

@@ -8,8 +8,9 @@ known-answer checks it has, on the GPU:
   actuation 0 must drift by at most 0.05 over 20,000 substeps;
 * the payload sink's documented size: helpers/payload_sink.py (centred
   payload, 60,000 substeps by default) measured a sink of 0.089
-  (experiments/EXPERIMENT_4.md:56); the same tank here sinks 0.0879 on the
-  batched path and 0.0867 on the plain path over 60,000 substeps.
+  (experiments/EXPERIMENT_4.md:56); the same tank here sinks 0.0847 on the
+  plain path and 0.0834 on the batched path over 60,000 substeps, means of
+  single runs that spread by an sd of about 0.004 (summation order).
 
 The payload tank is built here as evolve.py builds it (payload raster at
 2 points per cell, water lattice of spacing 1/256 minus a 0.005 margin around
@@ -105,19 +106,31 @@ def test_passive_centre_genome_barely_drifts():
 def test_payload_sink_matches_the_documented_value(path):
     """60,000 substeps of the centred payload tank (helpers/payload_sink.py's
     default run): the reference reports a sink of 0.089, quoted to two digits
-    from a Taichi FP32 run whose summation order and contraction differ; the
-    band is 15 %."""
+    from one Taichi FP32 run whose summation order and contraction differ.
+
+    One run is one draw from a spread: the order of the atomic P2G sums
+    changes from run to run and the payload's wake amplifies it, so single
+    60,000-substep sinks measured 0.078-0.091 on the plain path (6 runs, mean
+    0.0847, sd 0.0045) and 0.075-0.089 on the batched path (16 instances,
+    mean 0.0834, sd 0.0037).  The tank therefore runs as 8 identical
+    instances; their mean must lie within 15 % of 0.089 (its sd is about
+    0.0015) and every instance within 30 %."""
     from jellyfih_b200 import Engine, InstanceSpec
     payload, pos, mat, fib = _payload_tank(80000)
-    e = Engine([InstanceSpec(80000)], path=path)
+    copies = 8
+    e = Engine([InstanceSpec(80000)] * copies, path=path)
     try:
-        e.load(0, pos, mat, fib)
+        for m in range(copies):
+            e.load(m, pos, mat, fib)
         e.time = 0.0
-        y0 = e.payload_stats()[0, 0]
+        y0 = e.payload_stats()[:, 0]
         e.step(60000)
-        s = e.payload_stats()[0]
-        assert s[2] == len(payload) and not e.error_flags().any()
-        sink = y0 - s[0]
-        assert 0.089 * 0.85 <= sink <= 0.089 * 1.15, f"payload sank {sink:.4f}; the reference reports 0.089"
+        s = e.payload_stats()
+        assert (s[:, 2] == len(payload)).all() and not e.error_flags().any()
+        sinks = y0 - s[:, 0]
+        mean = float(sinks.mean())
+        assert 0.089 * 0.85 <= mean <= 0.089 * 1.15, \
+            f"payload sank {mean:.4f} on average ({np.round(sinks, 4)}); the reference reports 0.089"
+        assert ((sinks >= 0.089 * 0.7) & (sinks <= 0.089 * 1.3)).all(), f"single sinks {np.round(sinks, 4)}"
     finally:
         e.close()

@@ -95,3 +95,65 @@ def test_contiguous_partition_balances_and_covers():
         assert max(loads) <= sum(w) / parts + max(w)
     assert shard.contiguous_partition([1, 1], 4) == [(0, 1), (1, 2), (2, 2), (2, 2)]
     assert shard.contiguous_partition([], 2) == [(0, 0), (0, 0)]
+
+
+def _nccl_worker(port, q):
+    """One NCCL rank on cuda:0: the sharded headless run on real engines, the
+    row gather through NCCL (device tensors), and the scalar all-reduce the
+    benchmark uses for its max-over-ranks time."""
+    import torch
+    from jellyfih_b200 import Engine, InstanceSpec
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        inputs = _tank_inputs()
+        got = shard.run_headless_sharded(
+            lambda n: Engine([InstanceSpec(8000, 64, 64, 1.0)] * n, path="batched"), inputs, 20)
+        t = torch.tensor([3.5], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        q.put((dist.get_backend(), got, float(t.item())))
+    finally:
+        dist.destroy_process_group()
+
+
+def _tank_inputs():
+    from jellyfih_b200 import tank
+    out = []
+    for g in tank.uniform_genomes(3, 11):
+        pos, mat, fib, _ = tank.fill_tank(g, 8000, grid_res=64)
+        c, f = tank.timing_params(g)
+        out.append((pos, mat, fib, c, f))
+    return out
+
+
+@pytest.mark.gpu
+def test_sharded_headless_over_nccl_matches_one_engine():
+    """The NCCL branch of the result gather (rows staged on the GPU), run as a
+    one-rank NCCL group in a spawned process, against run_headless of one
+    engine holding every instance (the same substeps; rows agree to the
+    summation-order noise of 20 substeps)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jellyfih_b200 import Engine, InstanceSpec
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_worker, args=(_free_port(), q))
+    p.start()
+    backend, got, tmax = q.get(timeout=300)
+    p.join(timeout=60)
+    assert p.exitcode == 0 and backend == "nccl" and tmax == 3.5
+    inputs = _tank_inputs()
+    e = Engine([InstanceSpec(8000, 64, 64, 1.0)] * len(inputs), path="batched")
+    try:
+        for m, (pos, mat, fib, c, f) in enumerate(inputs):
+            e.load(m, pos, mat, fib)
+        e.set_params(contraction=[i[3] for i in inputs], freq=[i[4] for i in inputs])
+        ref = e.run_headless(20)
+    finally:
+        e.close()
+    assert got.shape == (len(inputs), 5)
+    np.testing.assert_array_equal(got[:, [0, 1, 4]], ref[:, [0, 1, 4]])
+    np.testing.assert_allclose(got[:, 2:4], ref[:, 2:4], rtol=0, atol=1e-6)

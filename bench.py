@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=32, help="instances per GPU")
     ap.add_argument("--slots", type=int, default=80000)
     ap.add_argument("--resort", type=int, default=64)
-    ap.add_argument("--block", type=int, default=512)
+    ap.add_argument("--block", type=int, default=768,
+                    help="threads per CTA of the chunk kernel (above 512: node blocks in TMEM)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the 256 x 64^2 gradient-refinement leg")

@@ -68,7 +68,9 @@ typedef struct {
   uint32_t flags;                       /* JF_FLAG_* */
   int32_t device;                       /* CUDA device ordinal */
   int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 64 */
-  int32_t block_threads;                /* batched: threads per CTA, 0 = 512 */
+  int32_t block_threads;                /* batched: threads per CTA (multiple of 32, <= 768),
+                                           0 = 768; above 512 the cell lanes keep their node
+                                           blocks in tensor memory (TMEM), up to 512 in registers */
   int32_t cluster_size;                 /* batched: CTAs per instance (1..16), 0 = automatic */
   int32_t cell_cap;                     /* batched: particles a cell lane accumulates per substep;
                                            the rest of the cell goes through per-particle atomics.

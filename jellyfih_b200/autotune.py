@@ -19,8 +19,10 @@ import itertools
 from .engine import Engine
 from ._lib import JfError
 
-# (block_threads, cell_cap); cell_cap 0 = chosen by the cost model at every re-sort
-LAYOUTS = ((512, 0), (384, 0), (512, 4))
+# (block_threads, cell_cap); cell_cap 0 = chosen by the cost model at every re-sort.
+# 768 threads keep the cell lanes' node blocks in TMEM (24 warps per SM), 512
+# in registers (16 warps per SM)
+LAYOUTS = ((768, 0), (512, 0), (768, 4))
 
 
 def autotune(specs, inputs, clusters=(0, 4, 8, 16), resorts=(16, 32, 64, 128), trial_steps=256,

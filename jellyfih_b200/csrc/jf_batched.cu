@@ -53,6 +53,8 @@ constexpr int kRowCost = 40;  // grid update of one row, in the cost model's uni
 // 2.3 % on the 32-instance batch against no weight).
 constexpr int kSolidCostHalves = 3;
 constexpr int kNoCap = 1 << 30;
+// CTA size of the TMEM variant of the chunk kernel (24 warps per SM)
+constexpr int kTmemThreads = 768;
 
 // Sort cell of a particle: (floor(X - 1/4), floor(Y - 1/4)) in grid units,
 // clamped at 0.  The stencil base trunc(X - 1/2) of a particle in sort cell k
@@ -129,6 +131,110 @@ __device__ __forceinline__ float2 dsmem_ld2(uint32_t a) {
   asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
   return v;
 }
+
+// Tensor memory (TMEM) variant of the cell lanes' node block.  With more than
+// 16 warps per SM the 48-float block no longer fits in registers beside one
+// particle's state, so between the particles of its cell a lane keeps the
+// block in TMEM: warp w of the CTA uses TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31
+// (its threads' own lanes, the quadrant a warp may access) and the 48 columns
+// starting at 48 (w / 4) of the CTA's allocation.  Each access starts at a
+// multiple of its width in columns.  A load first waits for the thread's
+// earlier stores (tcgen05.wait::st; the second half needs none of its own,
+// see the cell loop) and waits for its data inside the same asm statement, so
+// its outputs cannot be read before they arrive.
+#define JF_TM_OUT16(b)                                                                                   \
+  "=r"(r[b + 0]), "=r"(r[b + 1]), "=r"(r[b + 2]), "=r"(r[b + 3]), "=r"(r[b + 4]), "=r"(r[b + 5]),        \
+      "=r"(r[b + 6]), "=r"(r[b + 7]), "=r"(r[b + 8]), "=r"(r[b + 9]), "=r"(r[b + 10]), "=r"(r[b + 11]), \
+      "=r"(r[b + 12]), "=r"(r[b + 13]), "=r"(r[b + 14]), "=r"(r[b + 15])
+#define JF_TM_IN16(b)                                                                                             \
+  "r"(r[b + 0]), "r"(r[b + 1]), "r"(r[b + 2]), "r"(r[b + 3]), "r"(r[b + 4]), "r"(r[b + 5]), "r"(r[b + 6]),      \
+      "r"(r[b + 7]), "r"(r[b + 8]), "r"(r[b + 9]), "r"(r[b + 10]), "r"(r[b + 11]), "r"(r[b + 12]), "r"(r[b + 13]), \
+      "r"(r[b + 14]), "r"(r[b + 15])
+#define JF_TM_OUT8(b) \
+  "=r"(r[b + 0]), "=r"(r[b + 1]), "=r"(r[b + 2]), "=r"(r[b + 3]), "=r"(r[b + 4]), "=r"(r[b + 5]), "=r"(r[b + 6]), "=r"(r[b + 7])
+#define JF_TM_IN8(b) \
+  "r"(r[b + 0]), "r"(r[b + 1]), "r"(r[b + 2]), "r"(r[b + 3]), "r"(r[b + 4]), "r"(r[b + 5]), "r"(r[b + 6]), "r"(r[b + 7])
+
+// columns 0 .. 47 of the warp's block (the flush; the zeroing at a task's start)
+__device__ __forceinline__ void tm_load48(uint32_t ta, float* acc) {
+  uint32_t r[48];
+  asm volatile(
+      "tcgen05.wait::st.sync.aligned;\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%48];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%49];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47}, [%50];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : JF_TM_OUT16(0), JF_TM_OUT16(16), JF_TM_OUT16(32)
+      : "r"(ta), "r"(ta + 16u), "r"(ta + 32u)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 48; ++q) acc[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tm_zero48(uint32_t ta) {
+  const uint32_t z = 0u;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%1], {%3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%2], {%3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3, %3};"
+      :
+      : "r"(ta), "r"(ta + 16u), "r"(ta + 32u), "r"(z)
+      : "memory");
+}
+// columns 0 .. 23 (block rows 0 and 1): 16 at 0, 8 at 16
+__device__ __forceinline__ void tm_load_rows01(uint32_t ta, float* acc) {
+  uint32_t r[24];
+  asm volatile(
+      "tcgen05.wait::st.sync.aligned;\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%24];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16, %17, %18, %19, %20, %21, %22, %23}, [%25];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : JF_TM_OUT16(0), JF_TM_OUT8(16)
+      : "r"(ta), "r"(ta + 16u)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 24; ++q) acc[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tm_store_rows01(uint32_t ta, const float* acc) {
+  uint32_t r[24];
+#pragma unroll
+  for (int q = 0; q < 24; ++q) r[q] = __float_as_uint(acc[q]);
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%18, %19, %20, %21, %22, %23, %24, %25};"
+      :
+      : "r"(ta), "r"(ta + 16u), JF_TM_IN16(0), JF_TM_IN8(16)
+      : "memory");
+}
+// columns 24 .. 47 (block rows 2 and 3): 8 at 24, 16 at 32.  No wait for
+// earlier stores: the last store to these columns came before the wait of the
+// rows-0/1 load that precedes every use.
+__device__ __forceinline__ void tm_load_rows23(uint32_t ta, float* acc) {
+  uint32_t r[24];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%24];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23}, [%25];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : JF_TM_OUT8(0), JF_TM_OUT16(8)
+      : "r"(ta + 24u), "r"(ta + 32u)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 24; ++q) acc[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tm_store_rows23(uint32_t ta, const float* acc) {
+  uint32_t r[24];
+#pragma unroll
+  for (int q = 0; q < 24; ++q) r[q] = __float_as_uint(acc[q]);
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25};"
+      :
+      : "r"(ta + 24u), "r"(ta + 32u), JF_TM_IN8(0), JF_TM_IN16(8)
+      : "memory");
+}
+#undef JF_TM_OUT16
+#undef JF_TM_IN16
+#undef JF_TM_OUT8
+#undef JF_TM_IN8
 
 // the band (CTA of the cluster) that owns grid row j, and j's row in its window
 __device__ __forceinline__ int owner_of(const Window& w, int j) {
@@ -220,6 +326,40 @@ __device__ __forceinline__ void accumulate_block(float* acc, const JfInst& I, co
   }
 }
 
+// accumulate_block restricted to block rows J0 and J0 + 1, whose 24 floats
+// `acc` holds (the TMEM variant adds a particle half a block at a time).
+template <int J0>
+__device__ __forceinline__ void accumulate_rows(float* acc, const JfInst& I, const JfStencil& st,
+                                                const JfScatter& sc, int di, int dj) {
+  const bool sx = di != 0, sy = dj != 0;
+  const float wx4[4] = {sx ? 0.0f : st.wx0, sx ? st.wx0 : st.wx1, sx ? st.wx1 : st.wx2, sx ? st.wx2 : 0.0f};
+  const float wy4[4] = {sy ? 0.0f : st.wy0, sy ? st.wy0 : st.wy1, sy ? st.wy1 : st.wy2, sy ? st.wy2 : 0.0f};
+  const float ex = (float)di + st.fx0, ey = (float)dj + st.fx1;
+  float P[4], Q0[4], Q1[4], Pm[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float d0 = ((float)i - ex) * I.dx;
+    P[i] = wx4[i];
+    Q0[i] = wx4[i] * (sc.mv0 + sc.af00 * d0);
+    Q1[i] = wx4[i] * (sc.mv1 + sc.af10 * d0);
+    Pm[i] = wx4[i] * sc.mass;
+  }
+#pragma unroll
+  for (int jj = 0; jj < 2; ++jj) {
+    const int j = J0 + jj;
+    const float d1 = ((float)j - ey) * I.dx;
+    const float r0 = sc.af01 * d1, r1 = sc.af11 * d1;
+    const float wj = wy4[j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int q = (jj * 4 + i) * 3;
+      acc[q + 0] += wj * (Q0[i] + P[i] * r0);
+      acc[q + 1] += wj * (Q1[i] + P[i] * r1);
+      acc[q + 2] += wj * Pm[i];
+    }
+  }
+}
+
 // Writes a warp's 4x4 node blocks into the window.  Lane l owns cell column
 // cx = seg0 + l and covers node columns cx-1 .. cx+2; node column cx collects
 // block column 1 of lane l, 0 of lane l+1, 2 of lane l-1 and 3 of lane l-2,
@@ -257,7 +397,10 @@ __device__ __forceinline__ void flush_block(const float* acc, const Window& w, i
   }
 }
 
-__global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
+// kTmem: the node blocks live in TMEM (launched with 544 .. 768 threads, 80
+// registers at 768); otherwise in registers (up to 512 threads, 128 registers).
+template <bool kTmem>
+__global__ void __launch_bounds__(kTmem ? kTmemThreads : 512, 1) chunk_kernel(ChunkArgs a) {
   extern __shared__ float4 smem4[];
   float* sm = reinterpret_cast<float*>(smem4);
   // per-substep values, double-buffered so that substep s + 1's are set
@@ -308,9 +451,35 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
   const int32_t* __restrict__ mat_m = a.mat + p0;
 
   for (int n = tid; n < n_planes * WN; n += nth) sm[n] = 0.0f;
-  unsigned n_fast = 0, n_generic = 0, n_gather_generic = 0, n_overflow = 0;
+  // path counters of the CTA: register-block scatters, per-particle (generic)
+  // scatters, generic gathers, overflow particles
+  __shared__ unsigned s_path[4];
+  if (tid < 4) s_path[tid] = 0u;
   bool nonfinite = false;  // a G2P result of this thread's particles was NaN/Inf
+  // TMEM: 48 columns per warp of a lane quadrant, rounded up to a power of two
+  // (256 for up to 16 + 4 warps, 512 for 24); one CTA per SM, so the
+  // allocation never waits for another CTA's
+  __shared__ uint32_t s_tmem;
+  uint32_t tm_cols = 32, tm_base = 0, ta = 0;
+  if constexpr (kTmem) {
+    const int per_quad = (n_warps + 3) >> 2;
+    while (tm_cols < (uint32_t)(48 * per_quad)) tm_cols <<= 1;
+    __syncwarp();
+    if (warp == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                   "r"(tm_cols)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  }
   cluster.sync();
+  if constexpr (kTmem) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    tm_base = s_tmem;
+    ta = tm_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(48 * (warp >> 2));
+  }
 
   // G2P of the previous substep, then P2G of this one, for a particle that
   // is not handled by a cell lane (generic gathers and scatters).
@@ -390,8 +559,7 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         if (e < n_generic_all) {
           const bool over = e < n_ov;
           particle_generic(p0 + (over ? ov[e] : oor_beg + e - n_ov), do_g2p, do_p2g, pressure);
-          n_overflow += over ? 1u : 0u;
-          n_generic += over ? 0u : 1u;
+          atomicAdd(&s_path[over ? 3 : 1], 1u);
         }
         int nt = 0;
         if (lane == 0) nt = atomicAdd(next_task, 1);
@@ -408,17 +576,13 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         beg = cstart[c];
         end = min(cstart[c + 1], beg + cap);  // the rest of the cell is overflow
       }
-      // 4x4 node block: columns cx-1 .. cx+2, rows cy-1 .. cy+2
-      float acc[48];
-#pragma unroll
-      for (int q = 0; q < 48; ++q) acc[q] = 0.0f;
-      float4 nxv;
-      int nmt = -1;
-      if (beg < end) {
-        nxv = xv_m[beg];
-        nmt = mat_m[beg];
-      }
-      for (int k = beg; k < end; ++k) {
+      // G2P then P2G of particle k of this lane's cell (nxv / nmt: its
+      // prefetched position-velocity and material, replaced by particle
+      // k + 1's); returns true when its stencil lies in the lane's 4x4 node
+      // block (columns cx-1 .. cx+2, rows cy-1 .. cy+2), with the stencil,
+      // the scatter terms and the block offset for the caller to add
+      auto cell_particle = [&](int k, float4& nxv, int& nmt, JfStencil& st, JfScatter& sc, int& di,
+                               int& dj) -> bool {
         const float4 xv = nxv;
         const int mt = nmt;
         float4 F = F_m[k];  // first used by P2G, after the gather
@@ -433,21 +597,21 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         // C is read only where G2P does not run
         float4 C;
         if (do_g2p) {
-          JfStencil st;
-          if (!jf_stencil(I, x, st)) {
+          JfStencil gs;
+          if (!jf_stencil(I, x, gs)) {
             C = C_m[k];
           } else {
-            const int wr0 = st.by - w.win0;
+            const int wr0 = gs.by - w.win0;
             if (wr0 >= 0 && wr0 + 2 < w.VR) {
-              const int wb = wr0 * nx + st.bx;
-              jf_g2p_apic(I, st, v, C, [&](int i, int j) {
+              const int wb = wr0 * nx + gs.bx;
+              jf_g2p_apic(I, gs, v, C, [&](int i, int j) {
                 const int n = wb + j * nx + i;
                 return w.G[n];
               });
             } else {
-              ++n_gather_generic;
-              jf_g2p_apic(I, st, v, C,
-                          [&](int i, int j) { return gather_node(w, cluster, st.bx + i, st.by + j); });
+              atomicAdd(&s_path[2], 1u);
+              jf_g2p_apic(I, gs, v, C,
+                          [&](int i, int j) { return gather_node(w, cluster, gs.bx + i, gs.by + j); });
             }
           }
           jf_g2p_advect(I, x, v);
@@ -461,39 +625,97 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
         } else {
           C = C_m[k];
         }
-        if (do_p2g) {
+        if (!do_p2g) return false;
+        if (!jf_stencil(I, x, st)) {
+          if (do_g2p) C_m[k] = C;  // out of range: the next G2P keeps this C
+          return false;
+        }
+        const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
+        jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
+                        I.axisym ? a.rref[p0 + k] : 1.0f);
+        F_m[k] = F;
+        if (mt == 2) a.Jp[p0 + k] = jp;
+        di = st.bx - (cx - 1);
+        dj = st.by - (cy - 1);
+        if ((unsigned)di < 2u && (unsigned)dj < 2u) {
+          if (I.axisym) {  // the hoop sum goes straight to the window (rows in it)
+            const int hb = (st.by - w.win0) * nx + st.bx;
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+              for (int ii = 0; ii < 3; ++ii)
+                atomicAdd(w.Ah + hb + jj * nx + ii, jf_w(st, 0, ii) * jf_w(st, 1, jj) * sc.hoop);
+          }
+          return true;
+        }
+        atomicAdd(&s_path[1], 1u);
+        scatter_particle(w, cluster, I, st, sc);
+        return false;
+      };
+      float4 nxv;
+      int nmt = -1;
+      if (beg < end) {
+        nxv = xv_m[beg];
+        nmt = mat_m[beg];
+      }
+      if constexpr (!kTmem) {
+        // the lane's cell runs as a loop of its own length; the block stays in registers
+        unsigned n_block = 0;
+        float acc[48];
+#pragma unroll
+        for (int q = 0; q < 48; ++q) acc[q] = 0.0f;
+        for (int k = beg; k < end; ++k) {
           JfStencil st;
-          if (jf_stencil(I, x, st)) {
-            const float2 fb = (mt == 3) ? a.fiber[p0 + k] : make_float2(0.0f, 1.0f);
-            JfScatter sc;
-            jf_p2g_particle(I, mats, mt, v, C, F, jp, fb, pressure, P.payload_density, sc, x.x,
-                            I.axisym ? a.rref[p0 + k] : 1.0f);
-            F_m[k] = F;
-            if (mt == 2) a.Jp[p0 + k] = jp;
-            const int di = st.bx - (cx - 1), dj = st.by - (cy - 1);
-            const bool in_block = (unsigned)di < 2u && (unsigned)dj < 2u;
-            n_fast += in_block ? 1u : 0u;
-            n_generic += in_block ? 0u : 1u;
-            if (in_block) {
-              accumulate_block(acc, I, st, sc, di, dj);
-              if (I.axisym) {  // the hoop sum goes straight to the window (rows in it)
-                const int hb = (st.by - w.win0) * nx + st.bx;
-#pragma unroll
-                for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                  for (int ii = 0; ii < 3; ++ii)
-                    atomicAdd(w.Ah + hb + jj * nx + ii, jf_w(st, 0, ii) * jf_w(st, 1, jj) * sc.hoop);
-              }
-            } else {
-              scatter_particle(w, cluster, I, st, sc);
-            }
-          } else if (do_g2p) {
-            C_m[k] = C;  // out of range: the next G2P keeps this C
+          JfScatter sc;
+          int di, dj;
+          if (cell_particle(k, nxv, nmt, st, sc, di, dj)) {
+            accumulate_block(acc, I, st, sc, di, dj);
+            ++n_block;
           }
         }
+        __syncwarp();
+        if (do_p2g) {
+          flush_block(acc, w, lane, cx, cy, seg0, nx);
+          const unsigned nb = __reduce_add_sync(0xffffffffu, n_block);
+          if (lane == 0 && nb) atomicAdd(&s_path[0], nb);
+        }
+      } else {
+        // the warp steps its cells' particles together (the TMEM accesses are
+        // warp-wide) for as many iterations as its fullest cell; the block of
+        // each lane is loaded from TMEM, added to and stored back, two rows at
+        // a time, once per iteration in which some lane's particle adds to it
+        const int iters = (int)__reduce_max_sync(0xffffffffu, (unsigned)(end - beg));
+        __syncwarp();
+        if (do_p2g) tm_zero48(ta);
+        for (int it = 0; it < iters; ++it) {
+          const int k = beg + it;
+          JfStencil st;
+          JfScatter sc;
+          int di = 0, dj = 0;
+          const bool blk = k < end && cell_particle(k, nxv, nmt, st, sc, di, dj);
+          if (do_p2g) {
+            const unsigned bm = __ballot_sync(0xffffffffu, blk);
+            if (bm) {
+              if (lane == 0) atomicAdd(&s_path[0], (unsigned)__popc(bm));
+              float half[24];
+              tm_load_rows01(ta, half);
+              if (blk) accumulate_rows<0>(half, I, st, sc, di, dj);
+              __syncwarp();
+              tm_store_rows01(ta, half);
+              tm_load_rows23(ta, half);
+              if (blk) accumulate_rows<2>(half, I, st, sc, di, dj);
+              __syncwarp();
+              tm_store_rows23(ta, half);
+            }
+          }
+        }
+        __syncwarp();
+        if (do_p2g) {
+          float acc[48];
+          tm_load48(ta, acc);
+          flush_block(acc, w, lane, cx, cy, seg0, nx);
+        }
       }
-      __syncwarp();
-      if (do_p2g) flush_block(acc, w, lane, cx, cy, seg0, nx);
       int nt = 0;
       if (lane == 0) nt = atomicAdd(next_task, 1);
       task_id = __shfl_sync(0xffffffffu, nt, 0);
@@ -573,19 +795,18 @@ __global__ void __launch_bounds__(512, 1) chunk_kernel(ChunkArgs a) {
     }
   }
   if (__any_sync(0xffffffffu, nonfinite) && lane == 0) atomicOr(a.err + m, 1);
-  // path counters: one atomic per warp
-  if (a.path) {
-    const unsigned f = __reduce_add_sync(0xffffffffu, n_fast);
-    const unsigned g = __reduce_add_sync(0xffffffffu, n_generic);
-    const unsigned h = __reduce_add_sync(0xffffffffu, n_gather_generic);
-    const unsigned o = __reduce_add_sync(0xffffffffu, n_overflow);
-    if (lane == 0) {
-      atomicAdd(a.path + 0, (unsigned long long)f);
-      atomicAdd(a.path + 1, (unsigned long long)g);
-      atomicAdd(a.path + 2, (unsigned long long)h);
-      atomicAdd(a.path + 3, (unsigned long long)o);
+  // the CTA's path counters, and the TMEM allocation freed once every warp
+  // is past its last access
+  if constexpr (kTmem) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if constexpr (kTmem) {
+    if (warp == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm_base), "r"(tm_cols)
+                   : "memory");
     }
   }
+  if (a.path && tid < 4 && s_path[tid]) atomicAdd(a.path + tid, (unsigned long long)s_path[tid]);
   // peers may still read this CTA's grid rows in their last G2P pass
   cluster.sync();
 }
@@ -927,7 +1148,8 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   cudaError_t err;
   {
     JfTimed timed(e, false, e->capturing);
-    err = cudaLaunchKernelEx(&cfg, chunk_kernel, a);
+    err = e->block_threads > 512 ? cudaLaunchKernelEx(&cfg, chunk_kernel<true>, a)
+                                 : cudaLaunchKernelEx(&cfg, chunk_kernel<false>, a);
   }
   e->launches += 1;
   if (err != cudaSuccess) return err;
@@ -939,13 +1161,18 @@ static cudaError_t launch_chunk(jf_engine* e, int K) {
   return cudaGetLastError();
 }
 
+// the chunk kernel instantiation the engine's CTA size selects
+static const void* chunk_kernel_for(const jf_engine* e) {
+  return e->block_threads > 512 ? (const void*)chunk_kernel<true> : (const void*)chunk_kernel<false>;
+}
+
 cudaError_t jf_batched_prepare(jf_engine* e) {
   const size_t smem = jf_batched_smem_bytes(e);
-  cudaError_t err = cudaFuncSetAttribute(chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+  const void* k = chunk_kernel_for(e);
+  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   if (e->cluster > 8) {
-    err = cudaFuncSetAttribute(chunk_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    err = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (err != cudaSuccess) return err;
   }
   return cudaSuccess;
@@ -963,7 +1190,7 @@ int jf_batched_max_active_clusters(jf_engine* e, int cluster, int* out) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return (int)cudaOccupancyMaxActiveClusters(out, chunk_kernel, &cfg);
+  return (int)cudaOccupancyMaxActiveClusters(out, chunk_kernel_for(e), &cfg);
 }
 
 static cudaError_t chunk_with_sort(jf_engine* e, int K) {

@@ -257,7 +257,7 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
   e->path = cfg->path;
   e->flags = cfg->flags;
   e->resort_interval = cfg->resort_interval > 0 ? cfg->resort_interval : 64;
-  e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 512;
+  e->block_threads = cfg->block_threads > 0 ? cfg->block_threads : 768;
   e->cell_cap = cfg->cell_cap;
   e->use_graphs = (cfg->flags & JF_FLAG_NO_GRAPHS) == 0;
   auto bail = [&](int code, const std::string& msg) {
@@ -266,7 +266,8 @@ int jf_create(const jf_config* cfg, jf_engine** out) {
     return code;
   };
   if (cfg->cell_cap < 0) return bail(JF_ERR_INVALID, "cell_cap must be >= 0");
-  if (e->block_threads > 512 || e->block_threads % 32) return bail(JF_ERR_INVALID, "block_threads must be a multiple of 32, <= 512");
+  if (e->block_threads > 768 || e->block_threads % 32)
+    return bail(JF_ERR_INVALID, "block_threads must be a multiple of 32, <= 768");
 
   int ny_max = 0;
   for (int m = 0; m < e->M; ++m) {

@@ -40,7 +40,7 @@ struct jf_engine {
   int32_t path = JF_PATH_PLAIN;
   uint32_t flags = 0;
   int32_t resort_interval = 16;
-  int32_t block_threads = 512;
+  int32_t block_threads = 768;
   int32_t cluster = 4;
 
   std::vector<JfInst> inst;        // host copy

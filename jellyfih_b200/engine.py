@@ -51,7 +51,7 @@ class Engine:
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
-                 block_threads: int = 512, cluster_size: int = 0, graphs: bool = True,
+                 block_threads: int = 768, cluster_size: int = 0, graphs: bool = True,
                  cell_cap: int = 0, axisym: bool = False, grad_fp64: bool = False):
         self._lib = L.load()
         self.instances = list(instances)

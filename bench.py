@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--instances", type=int, default=32, help="instances per GPU")
     ap.add_argument("--slots", type=int, default=80000)
     ap.add_argument("--resort", type=int, default=64)
-    ap.add_argument("--block", type=int, default=768,
-                    help="threads per CTA of the chunk kernel (above 512: node blocks in TMEM)")
+    ap.add_argument("--block", type=int, default=0,
+                    help="threads per CTA of the chunk kernel (above 512: node blocks in TMEM); "
+                         "0 = the engine's choice")
     ap.add_argument("--no-extras", action="store_true", help="skip plain / e2e / CPU legs")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the 256 x 64^2 gradient-refinement leg")
@@ -620,6 +621,7 @@ def run_ours(args):
                     block_threads=args.block)
     stream = torch.cuda.Stream()
     engine.set_stream(stream)
+    layout = engine.layout()
     load_all(engine, inputs)
     engine.time = 0.0
 
@@ -744,7 +746,7 @@ def run_ours(args):
                                        f"FP32, {S} substeps per step",
                            "instances_per_gpu": M, "slots": args.slots, "live_particles": int(live_total),
                            "substeps_per_step": S, "resort_interval": args.resort,
-                           "block_threads": args.block,
+                           "block_threads": layout["block_threads"], "cluster_size": layout["cluster_size"],
                            "l2": "inputs larger than L2: particle state plus sort buffers ~260 MB per GPU",
                            "path": "batched"},
                 "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": gpu_launches,

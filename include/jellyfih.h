@@ -68,9 +68,11 @@ typedef struct {
   uint32_t flags;                       /* JF_FLAG_* */
   int32_t device;                       /* CUDA device ordinal */
   int32_t resort_interval;              /* batched: substeps between re-sorts, 0 = 64 */
-  int32_t block_threads;                /* batched: threads per CTA (multiple of 32, <= 768),
-                                           0 = 768; above 512 the cell lanes keep their node
-                                           blocks in tensor memory (TMEM), up to 512 in registers */
+  int32_t block_threads;                /* batched: threads per CTA (multiple of 32, <= 768); above
+                                           512 the cell lanes keep their node blocks in tensor
+                                           memory (TMEM), up to 512 in registers.  0 = 768 when the
+                                           tallest instance's bands hold >= 32 rows
+                                           (ceil(n_grid_y / cluster size)), else 512 */
   int32_t cluster_size;                 /* batched: CTAs per instance (1..16), 0 = automatic */
   int32_t cell_cap;                     /* batched: particles a cell lane accumulates per substep;
                                            the rest of the cell goes through per-particle atomics.
@@ -285,6 +287,11 @@ int jf_clear_error_flags(jf_engine* e);
  * their cell's per-lane cap, handed to the CTA's balanced overflow pass
  * (per-particle atomics).  All zero on the plain path. */
 int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset);
+
+/* The batched launch layout the engine chose: CTAs per instance (cluster
+ * size) and threads per CTA.  Either pointer may be NULL.  No counterpart in
+ * the reference (its launch layout is Taichi's). */
+int jf_get_layout(const jf_engine* e, int32_t* cluster_size, int32_t* block_threads);
 
 /* Largest grid, in nodes (n_grid * n_grid_y), jf_substep_noalloc accepts. */
 #define JF_NOALLOC_MAX_NODES 32768

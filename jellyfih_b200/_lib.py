@@ -95,6 +95,7 @@ EXPORTS = {
                                           ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                           ctypes.c_float] + [_P] * 9),
     "jf_path_counts": (ctypes.c_int, [_E, _P, ctypes.c_int32]),
+    "jf_get_layout": (ctypes.c_int, [_E, _P, _P]),
     "jf_set_kernel_timing": (ctypes.c_int, [_E, ctypes.c_int32]),
     "jf_kernel_timing": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int64),

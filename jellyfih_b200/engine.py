@@ -51,7 +51,7 @@ class Engine:
 
     def __init__(self, instances: Sequence[InstanceSpec], path: str = "batched", dt: float = DT,
                  glow: bool = False, device: int = 0, resort_interval: int = 64,
-                 block_threads: int = 768, cluster_size: int = 0, graphs: bool = True,
+                 block_threads: int = 0, cluster_size: int = 0, graphs: bool = True,
                  cell_cap: int = 0, axisym: bool = False, grad_fp64: bool = False):
         self._lib = L.load()
         self.instances = list(instances)
@@ -128,6 +128,13 @@ class Engine:
         self._check(self._lib.jf_path_counts(self._h, _ptr(out), 1 if reset else 0))
         return {"register_scatters": int(out[0]), "atomic_scatters": int(out[1]),
                 "remote_gathers": int(out[2]), "overflow_scatters": int(out[3])}
+
+    def layout(self) -> dict:
+        """The batched launch layout the engine chose: CTAs per instance and
+        threads per CTA (above 512 the cell lanes' node blocks live in TMEM)."""
+        cs, bt = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        self._check(self._lib.jf_get_layout(self._h, _ptr(cs), _ptr(bt)))
+        return {"cluster_size": int(cs[0]), "block_threads": int(bt[0])}
 
     def set_stream(self, stream) -> None:
         """Queue work on ``stream`` (a cudaStream_t as int, or a torch.cuda.Stream)."""

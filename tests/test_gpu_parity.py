@@ -20,6 +20,11 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 PATHS = ("plain", "batched")
+# the batched path's two chunk-kernel layouts: node blocks in registers (512
+# threads per CTA) and in tensor memory (768 threads); "batched" alone lets the
+# engine choose by band height
+LAYOUT_PATHS = ("plain", "batched_regs", "batched_tmem")
+BATCHED_LAYOUTS = ("batched_regs", "batched_tmem")
 FIELD_RTOL = 1e-5        # one substep: atomic summation order only
 MULTI_STEP_RTOL = 1e-4   # later checkpoints: order-only changes inside the oracle reach
                          # 2.7e-5 after 5 substeps of the perturbed fixture
@@ -35,7 +40,13 @@ def _gpu():
 
 def _engine(specs, path, **kw):
     from jellyfih_b200 import Engine
-    return Engine(specs, path=path, **kw)
+    if path in BATCHED_LAYOUTS:
+        kw.setdefault("block_threads", 512 if path == "batched_regs" else 768)
+        path = "batched"
+    e = Engine(specs, path=path, **kw)
+    if "block_threads" in kw and path == "batched":
+        assert e.layout()["block_threads"] == kw["block_threads"]
+    return e
 
 
 def _spec(d):
@@ -101,19 +112,20 @@ def _check_goldens(case, path, **kw):
     return counts
 
 
-@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("path", LAYOUT_PATHS)
 @pytest.mark.parametrize("case", G.STEP_CASES)
 def test_substeps_match_reference_goldens(case, path):
     _check_goldens(case, path)
 
 
+@pytest.mark.parametrize("layout", BATCHED_LAYOUTS)
 @pytest.mark.parametrize("cap", (1, 2, 16))
 @pytest.mark.parametrize("case", G.STEP_CASES)
-def test_cell_cap_overflow_matches_reference_goldens(case, cap):
+def test_cell_cap_overflow_matches_reference_goldens(case, cap, layout):
     """A cell lane accumulates at most `cap` particles; the rest of each cell
     goes through the per-band overflow list (per-particle atomics).  Caps 1
     and 2 push most particles through that list; 16 disables it."""
-    counts = _check_goldens(case, "batched", cell_cap=cap)
+    counts = _check_goldens(case, layout, cell_cap=cap)
     if cap == 1:
         assert counts["overflow_scatters"] > 0
     if cap == 16:
@@ -182,7 +194,7 @@ def _small_cluster(n_slots):
     return pos, mat, fib
 
 
-@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("path", LAYOUT_PATHS)
 def test_degenerate_instances_match_oracle(path):
     """Instances with nothing to step beside a full tank: all slots dead,
     water only (no payload and no body: zero CoM rows, as the reference
@@ -235,7 +247,8 @@ def test_degenerate_instances_match_oracle(path):
     e.close()
 
 
-def test_batched_odd_grids_against_oracle():
+@pytest.mark.parametrize("layout", BATCHED_LAYOUTS)
+def test_batched_odd_grids_against_oracle(layout):
     """Grid widths that are not multiples of 32 and do not divide the block
     (80 x 112 and 96 x 96 nodes): partial 32-cell segments, the generic grid
     update loop and uneven band heights, against the oracle after 1 and 5
@@ -251,7 +264,7 @@ def test_batched_odd_grids_against_oracle():
         c, f = tank.timing_params(g)
         specs.append(InstanceSpec(30000, nx, ny, dh))
         data.append((pos, mat, fib, c, f))
-    e = _engine(specs, "batched", resort_interval=2)
+    e = _engine(specs, layout, resort_interval=2)
     for m, (pos, mat, fib, c, f) in enumerate(data):
         e.load(m, pos, mat, fib)
     e.set_params(contraction=[d[3] for d in data], freq=[d[4] for d in data])
@@ -305,7 +318,8 @@ def test_full_tank_1000_steps_against_oracle(path):
     e.close()
 
 
-def test_batched_uneven_instances_against_oracle():
+@pytest.mark.parametrize("layout", BATCHED_LAYOUTS)
+def test_batched_uneven_instances_against_oracle(layout):
     """Mixed 128^2 / 128x256 / 64^2 instances in one batched launch, 200 substeps."""
     from jellyfih_b200 import InstanceSpec, tank
     cases = [dict(seed=21), dict(seed=22, n_slots=60000),
@@ -317,7 +331,7 @@ def test_batched_uneven_instances_against_oracle():
         specs.append(InstanceSpec(cfg.get("n_slots", 80000), cfg.get("grid", 128), cfg.get("ny", 128),
                                   cfg.get("dh", 1.0)))
         data.append((pos, mat, fib, c, f))
-    e = _engine(specs, "batched", resort_interval=8)
+    e = _engine(specs, layout, resort_interval=8)
     acts = np.array([500.0, 900.0, 700.0, 300.0], np.float32)
     for m, (pos, mat, fib, c, f) in enumerate(data):
         e.load(m, pos, mat, fib)
@@ -346,7 +360,8 @@ def test_resort_interval_and_drift_beyond_halo():
     live = mat >= 0
     v[live] = rng.normal(0, 10.0, (live.sum(), 2)).astype(np.float32)  # up to ~5 rows in 64 substeps
     outs = {}
-    for path, ri in (("plain", 16), ("batched", 1), ("batched", 64)):
+    for path, ri in (("plain", 16), ("batched_regs", 1), ("batched_regs", 64), ("batched_tmem", 1),
+                     ("batched_tmem", 64)):
         e = _engine([InstanceSpec(80000)], path, resort_interval=ri)
         e.load(0, pos, mat, fib)
         e.write(0, v=v)
@@ -356,10 +371,29 @@ def test_resort_interval_and_drift_beyond_halo():
         assert not e.error_flags().any()
         e.close()
     ref = outs[("plain", 16)]
-    for key in (("batched", 1), ("batched", 64)):
+    for key in [k for k in outs if k[0] != "plain"]:
         got = outs[key]
         assert np.abs(got["x"][live] - ref["x"][live]).max() < 1e-4, key
         assert_norm_close(got["v"][live], ref["v"][live], 1e-2, f"{key} v")
+
+
+def test_engine_layout_choice_and_limits():
+    """The engine's default CTA size: 768 threads (node blocks in TMEM) when the
+    bands hold >= 32 rows, 512 (registers) otherwise; sizes above 768 or not a
+    multiple of 32 are rejected before any launch."""
+    from jellyfih_b200 import Engine, InstanceSpec, _lib
+    e = Engine([InstanceSpec(1000)] * 32, path="batched")
+    assert e.layout() == {"cluster_size": 4, "block_threads": 768}  # 128 rows / 4 = 32
+    e.close()
+    e = Engine([InstanceSpec(1000, 64, 64, 1.0)] * 32, path="batched")
+    assert e.layout() == {"cluster_size": 4, "block_threads": 512}  # 64 rows / 4 = 16
+    e.close()
+    e = Engine([InstanceSpec(1000, 128, 256, 2.0)] * 16, path="batched")
+    assert e.layout() == {"cluster_size": 8, "block_threads": 768}  # 256 rows / 8 = 32
+    e.close()
+    for bad in (800, 100, -32):
+        with pytest.raises(_lib.JfError):
+            Engine([InstanceSpec(1000)], path="batched", block_threads=bad)
 
 
 def test_nonfinite_flag_and_invalid_arguments():
@@ -488,7 +522,7 @@ def test_gpu_fitness_matches_host_restatement():
 
 
 
-@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("path", LAYOUT_PATHS)
 def test_axisym_tall_scene_first_substeps_match_oracle(path):
     """The reference's axisymmetric scene (half-profile jellyfish, 128x256 tall
     tank, 160K slots, make_jelly.py:275-307) for its first two substeps,

@@ -155,21 +155,7 @@ __device__ __forceinline__ float2 dsmem_ld2(uint32_t a) {
 #define JF_TM_IN8(b) \
   "r"(r[b + 0]), "r"(r[b + 1]), "r"(r[b + 2]), "r"(r[b + 3]), "r"(r[b + 4]), "r"(r[b + 5]), "r"(r[b + 6]), "r"(r[b + 7])
 
-// columns 0 .. 47 of the warp's block (the flush; the zeroing at a task's start)
-__device__ __forceinline__ void tm_load48(uint32_t ta, float* acc) {
-  uint32_t r[48];
-  asm volatile(
-      "tcgen05.wait::st.sync.aligned;\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%48];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%49];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47}, [%50];\n\t"
-      "tcgen05.wait::ld.sync.aligned;"
-      : JF_TM_OUT16(0), JF_TM_OUT16(16), JF_TM_OUT16(32)
-      : "r"(ta), "r"(ta + 16u), "r"(ta + 32u)
-      : "memory");
-#pragma unroll
-  for (int q = 0; q < 48; ++q) acc[q] = __uint_as_float(r[q]);
-}
+// columns 0 .. 47 of the warp's block set to zero (a task's start)
 __device__ __forceinline__ void tm_zero48(uint32_t ta) {
   const uint32_t z = 0u;
   asm volatile(
@@ -365,19 +351,22 @@ __device__ __forceinline__ void accumulate_rows(float* acc, const JfInst& I, con
 // block column 1 of lane l, 0 of lane l+1, 2 of lane l-1 and 3 of lane l-2,
 // so each lane issues one atomic per (row, component).  Lane 0 also writes
 // column seg0-1, lane 31 columns seg0+32 and seg0+33.
+// `acc` holds block rows J0 .. J0 + NJ - 1 (the TMEM variant flushes two rows
+// at a time).
+template <int J0 = 0, int NJ = 4>
 __device__ __forceinline__ void flush_block(const float* acc, const Window& w, int lane, int cx, int cy,
                                             int seg0, int nx) {
   const unsigned full = 0xffffffffu;
 #pragma unroll
-  for (int J = 0; J < 4; ++J) {
+  for (int J = J0; J < J0 + NJ; ++J) {
     const int rowo = (cy - 1 + J - w.win0) * nx;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       float* A = q == 0 ? w.Ax : (q == 1 ? w.Ay : w.Am);
-      const float a0 = acc[(J * 4 + 0) * 3 + q];
-      const float a1 = acc[(J * 4 + 1) * 3 + q];
-      const float a2 = acc[(J * 4 + 2) * 3 + q];
-      const float a3 = acc[(J * 4 + 3) * 3 + q];
+      const float a0 = acc[((J - J0) * 4 + 0) * 3 + q];
+      const float a1 = acc[((J - J0) * 4 + 1) * 3 + q];
+      const float a2 = acc[((J - J0) * 4 + 2) * 3 + q];
+      const float a3 = acc[((J - J0) * 4 + 3) * 3 + q];
       const float from_right = __shfl_down_sync(full, a0, 1);
       const float from_left = __shfl_up_sync(full, a2, 1);
       const float from_left2 = __shfl_up_sync(full, a3, 2);
@@ -685,6 +674,7 @@ __global__ void __launch_bounds__(kTmem ? kTmemThreads : 512, 1) chunk_kernel(Ch
         // each lane is loaded from TMEM, added to and stored back, two rows at
         // a time, once per iteration in which some lane's particle adds to it
         const int iters = (int)__reduce_max_sync(0xffffffffu, (unsigned)(end - beg));
+        unsigned n_block = 0;  // the same in every lane of the warp
         __syncwarp();
         if (do_p2g) tm_zero48(ta);
         for (int it = 0; it < iters; ++it) {
@@ -696,7 +686,7 @@ __global__ void __launch_bounds__(kTmem ? kTmemThreads : 512, 1) chunk_kernel(Ch
           if (do_p2g) {
             const unsigned bm = __ballot_sync(0xffffffffu, blk);
             if (bm) {
-              if (lane == 0) atomicAdd(&s_path[0], (unsigned)__popc(bm));
+              n_block += (unsigned)__popc(bm);
               float half[24];
               tm_load_rows01(ta, half);
               if (blk) accumulate_rows<0>(half, I, st, sc, di, dj);
@@ -711,9 +701,13 @@ __global__ void __launch_bounds__(kTmem ? kTmemThreads : 512, 1) chunk_kernel(Ch
         }
         __syncwarp();
         if (do_p2g) {
-          float acc[48];
-          tm_load48(ta, acc);
-          flush_block(acc, w, lane, cx, cy, seg0, nx);
+          // the last store to columns 24 .. 47 precedes the wait of the first load
+          float half[24];
+          tm_load_rows01(ta, half);
+          flush_block<0, 2>(half, w, lane, cx, cy, seg0, nx);
+          tm_load_rows23(ta, half);
+          flush_block<2, 2>(half, w, lane, cx, cy, seg0, nx);
+          if (lane == 0 && n_block) atomicAdd(&s_path[0], n_block);
         }
       }
       int nt = 0;

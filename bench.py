@@ -164,12 +164,14 @@ def peaks():
 
 def traffic_per_particle_step():
     """DRAM bytes per live particle-substep of the chunk kernel from the
-    committed ncu measurement, or None when the kernel's sources changed since
-    that measurement (the file records a hash of them)."""
+    committed ncu measurement, and the measurement's record.  The figure is
+    None when the kernel's sources changed since that measurement (the file
+    records a hash of them); the record still names the figure and the sources
+    it was measured on."""
     import hashlib
     p = os.path.join(HERE, "profiles", "traffic.json")
     if not os.path.exists(p):
-        return None
+        return None, None
     with open(p) as f:
         d = json.load(f)
     h = hashlib.sha256()
@@ -177,8 +179,8 @@ def traffic_per_particle_step():
         with open(os.path.join(HERE, src), "rb") as f:
             h.update(f.read())
     if h.hexdigest()[:16] != d.get("kernel_sources_sha256_16"):
-        return None
-    return d.get("chunk_kernel_dram_bytes_per_live_particle_substep")
+        return None, d
+    return d.get("chunk_kernel_dram_bytes_per_live_particle_substep"), d
 
 
 def cpu_baseline(inputs, target_s=12.0):
@@ -659,7 +661,7 @@ def run_ours(args):
     bytes_per_launch = live * chunk_substeps * ALGO_BYTES
     mean_launch_s = kt["step_ms"] / max(kt["step_launches"], 1) / 1e3
     achieved = bytes_per_launch / mean_launch_s / 1e9
-    tpps = traffic_per_particle_step()
+    tpps, trec = traffic_per_particle_step()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": (tpps * live * chunk_substeps) if tpps else None,
@@ -668,6 +670,15 @@ def run_ours(args):
                 "step_kernel_share": kt["step_ms"] / ms if ms > 0 else None,
                 "scatter_paths": paths,
                 "sort_ms": kt["sort_ms"], "sort_launches": kt["sort_launches"]}
+    if tpps is None and trec is not None:
+        # the kernel changed since the ncu measurement: no traffic figure for this
+        # source, but the last measured one, scaled to this launch, and the sources
+        # it belongs to
+        last = trec.get("chunk_kernel_dram_bytes_per_live_particle_substep")
+        roofline["traffic_last_measured"] = {
+            "bytes_per_launch": last * live * chunk_substeps if last else None,
+            "kernel_sources_sha256_16": trec.get("kernel_sources_sha256_16"),
+            "note": "ncu figure of an earlier revision of the chunk kernel's sources"}
 
     extras = {}
     if world > 1 and args.gpus != world:

@@ -23,7 +23,7 @@
 // frequency moves the instant of the drop, and the loss moves with it.  The
 // backward therefore records dL/dpressure of every substep and adds, for every
 // drop inside the rollout, the boundary term of the time integral:
-// dL/dc += A g* / (f dt) and dL/df -= A g* t* / (f^2 dt) (t* the instant of
+// dL/dc += A g* / (f dt) and dL/df -= A g* t* / (f dt) (t* the instant of
 // the drop, g* dL/dpressure there, interpolated between the substeps around
 // it; a(c-) = 1).
 //

@@ -80,6 +80,15 @@ def parse():
     return ap.parse_args()
 
 
+def host_cores():
+    """Host cores this process may run on (its CPU affinity where the platform
+    reports it, else the machine's count)."""
+    try:
+        return len(os.sched_getaffinity(0)) or 1
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def make_inputs(M, slots, seed):
     from jellyfih_b200 import tank
     genomes = tank.gaussian_genomes(M, seed)
@@ -185,8 +194,8 @@ def traffic_per_particle_step():
 
 def cpu_baseline(inputs, target_s=12.0):
     """The CPU oracle on all host cores (OpenMP over instances), a bounded sample."""
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    cores = host_cores()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
     from oracle import oracle as O
     insts, states = [], []
     for pos, mat, fib, c, f, st in inputs:
@@ -554,8 +563,11 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    # rank 0 runs alone, on every core this process may use: torchrun's default
+    # OMP_NUM_THREADS=1 for its ranks is overridden (the oracle's OpenMP runtime
+    # reads the variable when the library is loaded, below)
+    cores = host_cores()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
     from oracle import oracle as O
     inputs = make_inputs(args.instances, args.slots, 1000)
     insts = [O.Instance(contraction=i[3], freq=i[4]) for i in inputs]

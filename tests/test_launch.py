@@ -44,3 +44,28 @@ def test_rank_environment():
     env = launch.rank_env(1, 4, 12345, base={})
     assert env == {"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "4", "LOCAL_WORLD_SIZE": "4",
                    "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": "12345"}
+
+
+def test_reference_arm_uses_every_core_under_torchrun_and_only_on_rank_0():
+    """bench.py --impl reference at N = 2 under torchrun's environment
+    (OMP_NUM_THREADS=1 for every rank): rank 0 prints the one line and times the
+    oracle on all of its cores; rank 1 exits 0 without output."""
+    import subprocess
+    import sys
+    bench = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "bench.py")
+    argv = [sys.executable, bench, "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0",
+            "--instances", "1", "--substeps", "2"]
+    cores = len(os.sched_getaffinity(0))
+    outs = []
+    for rank in (0, 1):
+        env = launch.rank_env(rank, 2, 29500)
+        env["OMP_NUM_THREADS"] = "1"
+        p = subprocess.run(argv, env=env, capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr[-2000:]
+        outs.append([ln for ln in p.stdout.splitlines() if ln.strip()])
+    assert outs[1] == []
+    assert len(outs[0]) == 1
+    d = json.loads(outs[0][0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2
+    assert d["cpu_baseline"]["cores"] == cores
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]

@@ -8,7 +8,11 @@
 * every shared-memory index chunk_kernel forms from such a layout stays in
   its window: the register-block flush rows, the halo push / pull rows and
   their owners' rows, the remote rows of generic scatters and gathers, and
-  the grid-update rows.
+  the grid-update rows;
+* the TMEM node blocks of chunk_kernel<true> (544 .. 768 threads): every
+  warp's 48 columns lie inside the CTA's allocation, warps of one lane
+  quadrant never share a column, and every tcgen05.ld / tcgen05.st starts at
+  a multiple of its width in columns.
 """
 import numpy as np
 import pytest
@@ -131,3 +135,42 @@ def test_fixed_bands_are_valid():
         band_h = (ny + cs - 1) // cs
         brow = [min(r * band_h, ny) for r in range(cs)] + [ny]
         check_layout(brow, ny, band_h)
+
+
+# tcgen05 accesses of one warp's block, relative to its first column
+# (tm_zero48, tm_load_rows01 / tm_store_rows01, tm_load_rows23 / tm_store_rows23):
+# (column offset, width in columns)
+TMEM_ACCESSES = [(0, 16), (16, 16), (32, 16),  # zero
+                 (0, 16), (16, 8),             # block rows 0 and 1
+                 (24, 8), (32, 16)]            # block rows 2 and 3
+
+
+def tmem_layout(n_warps):
+    """chunk_kernel<true>'s allocation (a power of two >= 32 columns covering
+    48 columns per warp of a lane quadrant) and warp w's (lane quadrant, first
+    column)."""
+    per_quad = (n_warps + 3) >> 2
+    cols = 32
+    while cols < 48 * per_quad:
+        cols <<= 1
+    return cols, [(w & 3, 48 * (w >> 2)) for w in range(n_warps)]
+
+
+@pytest.mark.parametrize("threads", range(544, 769, 32))
+def test_tmem_node_blocks_fit_and_are_aligned(threads):
+    n_warps = threads // 32
+    cols, warps = tmem_layout(n_warps)
+    assert cols in (256, 512)  # tcgen05.alloc: a power of two, 32 .. 512 columns
+    used = {}
+    for w, (quad, base) in enumerate(warps):
+        assert 0 <= quad < 4  # lanes 32 quad .. 32 quad + 31 of 128
+        for off, width in TMEM_ACCESSES:
+            start = base + off
+            assert start % width == 0, (w, off, width)
+            assert start + width <= cols, (w, off, width)
+        for c in range(base, base + 48):
+            assert (quad, c) not in used, (w, used.get((quad, c)))
+            used[(quad, c)] = w
+    # the accesses of one block cover exactly its 48 columns
+    load_store = TMEM_ACCESSES[3:]
+    assert sorted(c for off, width in load_store for c in range(off, off + width)) == list(range(48))

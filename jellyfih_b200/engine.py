@@ -37,6 +37,17 @@ def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
+_PATHS = {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}
+_FITNESS_MODES = {"efficiency": 0, "displacement": 1}
+
+
+def _choice(table, value, what):
+    try:
+        return table[value]
+    except (KeyError, TypeError):
+        raise ValueError(f"unknown {what} {value!r}; expected one of {sorted(table)}") from None
+
+
 class Engine:
     """A batch of independent MLS-MPM instances on one GPU.
 
@@ -61,7 +72,7 @@ class Engine:
             L.JfInstanceDesc(s.n_slots, s.n_grid, s.n_grid_y, s.domain_height) for s in self.instances])
         flags = ((L.JF_FLAG_GLOW if glow else 0) | (0 if graphs else L.JF_FLAG_NO_GRAPHS)
                  | (L.JF_FLAG_AXISYM if axisym else 0) | (L.JF_FLAG_GRAD_FP64 if grad_fp64 else 0))
-        cfg = L.JfConfig(self.M, descs, dt, {"plain": L.JF_PATH_PLAIN, "batched": L.JF_PATH_BATCHED}[path],
+        cfg = L.JfConfig(self.M, descs, dt, _choice(_PATHS, path, "path"),
                          flags, device, resort_interval, block_threads, cluster_size, cell_cap)
         h = L._E()
         rc = self._lib.jf_create(ctypes.byref(cfg), ctypes.byref(h))
@@ -218,7 +229,7 @@ class Engine:
         con = None if contraction is None else np.ascontiguousarray(contraction, dtype=np.float64).reshape(self.M)
         out = np.zeros(self.M, np.float64)
         self._check(self._lib.jf_fitness(self._h, _ptr(rows), _ptr(mus), _ptr(con),
-                                         {"efficiency": 0, "displacement": 1}[mode], _ptr(out)))
+                                         _choice(_FITNESS_MODES, mode, "fitness mode"), _ptr(out)))
         return out
 
     def run_episode(self, positions, materials, contraction, steps: int, fibers=None, freq=None,
@@ -243,7 +254,7 @@ class Engine:
         rows = np.zeros((self.M, 5), np.float64)
         fit = None if mus is None else np.zeros(self.M, np.float64)
         self._check_run(self._lib.jf_run_episode(self._h, _ptr(pos), _ptr(mat), _ptr(fib), _ptr(con), _ptr(frq),
-                                                 int(steps), _ptr(mus), {"efficiency": 0, "displacement": 1}[mode],
+                                                 int(steps), _ptr(mus), _choice(_FITNESS_MODES, mode, "fitness mode"),
                                                  _ptr(rows), _ptr(fit)))
         return rows, fit
 

@@ -83,3 +83,9 @@ def test_struct_layout():
     assert ctypes.sizeof(L.JfInstanceDesc) == 16
     assert L.JfConfig.instances.offset == 8 and L.JfConfig.dt.offset == 16
     assert ctypes.sizeof(L.JfConfig) == 56
+
+
+def test_engine_rejects_unknown_path_before_touching_the_device(lib):
+    from jellyfih_b200 import Engine, InstanceSpec
+    with pytest.raises(ValueError, match="unknown path 'gpu'"):
+        Engine([InstanceSpec(16)], path="gpu")

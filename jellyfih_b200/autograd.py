@@ -4,7 +4,11 @@
 loads every instance from `positions`, runs `steps` substeps with checkpoints
 (jf_grad_forward) and returns the (M,) payload CoM displacement as a tensor;
 its backward calls the hand-written adjoint kernels (jf_grad_backward,
-jf_grad_positions).  `refine_timing_genes` takes gradient steps on the two
+jf_grad_positions).  The engine keeps the checkpoints of its latest rollout
+only, so a rollout's backward runs before the next rollout on the same engine
+(grad_forward, grad_step or another forward here); a later backward raises
+RuntimeError instead of differentiating the wrong rollout.
+`refine_timing_genes` takes gradient steps on the two
 actuation-timing genes (contraction fraction, frequency multiplier) beside
 CMA-ES, as an optional refinement, each step's forward and backward replayed
 as one CUDA graph (jf_grad_step).
@@ -31,6 +35,7 @@ class RolloutDisplacement(torch.autograd.Function):
         engine.time = t0
         loss = engine.grad_forward(int(steps), int(checkpoint_every))
         ctx.engine = engine
+        ctx.rollout = engine.rollouts
         ctx.shape = positions.shape
         ctx.device = positions.device
         return torch.from_numpy(loss).to(actuation.device)
@@ -38,6 +43,10 @@ class RolloutDisplacement(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gout):
         e = ctx.engine
+        if e.rollouts != ctx.rollout:
+            # the engine keeps the checkpoints of its latest rollout only
+            raise RuntimeError("the engine ran another differentiable rollout after this one's forward; "
+                               "run the backward of a rollout before the next forward on the same engine")
         g = e.grad_backward()
         go = gout.detach().to("cpu", torch.float64).numpy()
         gx = np.stack([e.grad_positions(m) for m in range(e.M)]).astype(np.float64)

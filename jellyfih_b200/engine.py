@@ -81,6 +81,8 @@ class Engine:
         self._h = h
         self.dt = dt
         self.nonfinite_message = ""  # set when a run reported a non-finite particle state
+        self.rollouts = 0  # differentiable rollouts run (grad_forward / grad_step); a backward
+        # differentiates the latest one
         self.config = dict(path=path, resort_interval=resort_interval, block_threads=block_threads,
                            cluster_size=cluster_size, graphs=graphs, cell_cap=cell_cap, axisym=axisym)
 
@@ -265,6 +267,7 @@ class Engine:
         fixed-point P2G) is recorded as for run_headless: error_flags() names
         it, and its loss and gradients are not to be used."""
         loss = np.zeros(self.M, np.float64)
+        self.rollouts += 1
         self._check_run(self._lib.jf_grad_forward(self._h, int(steps), int(checkpoint_every), _ptr(loss)))
         return loss
 
@@ -281,6 +284,7 @@ class Engine:
         calls with the same sizes and start time); returns (loss, gradients)."""
         loss = np.zeros(self.M, np.float64)
         g = {k: np.zeros(self.M, np.float64) for k in ("actuation", "contraction", "freq")}
+        self.rollouts += 1
         self._check_run(self._lib.jf_grad_step(self._h, int(steps), int(checkpoint_every), _ptr(loss),
                                                _ptr(g["actuation"]), _ptr(g["contraction"]), _ptr(g["freq"])))
         return loss, g

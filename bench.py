@@ -202,10 +202,18 @@ def cpu_baseline(inputs, target_s=12.0):
         insts.append(O.Instance(contraction=c, freq=f))
         states.append(O.new_state(pos, mat, fib))
     live = sum(int((i[1] >= 0).sum()) for i in inputs)
-    t0 = time.perf_counter()
+    # two untimed substeps first (page faults on the fresh states, the OpenMP
+    # pool's start); then a short probe and one of about a tenth of the sample
+    # (every call also pays a fixed cost, which a short probe overstates) size
+    # the timed sample, one call of ~target_s
     t = O.run_batch(insts, states, np.float32(0), 2)
-    probe = time.perf_counter() - t0
-    n = int(max(2, min(2000, target_s / max(probe / 2, 1e-6))))
+    n = 2
+    for _ in range(2):
+        t0 = time.perf_counter()
+        t = O.run_batch(insts, states, t, n)
+        per = (time.perf_counter() - t0) / n
+        n = int(max(2, min(200, 0.1 * target_s / max(per, 1e-6))))
+    n = int(max(2, min(2000, target_s / max(per, 1e-6))))
     t0 = time.perf_counter()
     O.run_batch(insts, states, t, n)
     el = time.perf_counter() - t0

@@ -889,7 +889,8 @@ int jf_grad_step(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* 
 
 int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, double* d_freq) {
   if (check_engine(e)) return JF_ERR_INVALID;
-  if (!e->grad) return fail(e, JF_ERR_INVALID, "jf_grad_backward needs a jf_grad_forward first");
+  if (!jf_grad_done(e, 1))
+    return fail(e, JF_ERR_INVALID, "jf_grad_backward needs a completed jf_grad_forward first");
   int rc = set_device(e);
   if (rc) return rc;
   std::vector<double> g(3 * (size_t)e->M);
@@ -907,7 +908,9 @@ int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, d
 int jf_grad_positions(jf_engine* e, int32_t m, float* dx0) {
   if (check_engine(e) || !dx0) return JF_ERR_INVALID;
   if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
-  if (!e->grad) return fail(e, JF_ERR_INVALID, "jf_grad_positions needs a jf_grad_backward first");
+  if (!jf_grad_done(e, 2))
+    return fail(e, JF_ERR_INVALID,
+                "jf_grad_positions needs the backward of the latest rollout (jf_grad_backward or jf_grad_step)");
   int rc = set_device(e);
   if (rc) return rc;
   std::vector<float4> lx;

@@ -153,6 +153,7 @@ cudaError_t jf_grad_backward_impl(jf_engine* e, double* gparam_host);
 cudaError_t jf_grad_step_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode,
                               const double* inv_n, double* gparam_host);
 cudaError_t jf_grad_x0_impl(jf_engine* e, int m, std::vector<float4>& out);
+bool jf_grad_done(const jf_engine* e, int stage);
 void jf_grad_free(jf_engine* e);
 // The rollout's loss sums into e->d_stats (from the FP64 final state in the FP64 build).
 cudaError_t jf_grad_loss_stats(jf_engine* e);

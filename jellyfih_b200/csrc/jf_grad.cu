@@ -782,7 +782,8 @@ struct GradBuffers {
   cudaEvent_t fork = nullptr, join = nullptr;
   int32_t* body_mode = nullptr;
   double* inv_n = nullptr;
-  bool have_forward = false;
+  bool have_forward = false;   // the latest rollout's forward completed
+  bool have_backward = false;  // and its backward (the adjoint in lxv, lC, lF)
   int n_sm = 148;
   GradGraph fwd_graph, bwd_graph, step_graph;  // forward, backward, forward + backward
 
@@ -1331,6 +1332,7 @@ std::vector<uint64_t> graph_key(jf_engine* e, int tag) {
 
 template <class R>
 cudaError_t grad_begin(jf_engine* e, int64_t steps, int32_t K, const int32_t* body_mode, const double* inv_n) {
+  if (e->grad) bufs<R>(e).have_forward = bufs<R>(e).have_backward = false;  // a new rollout
   cudaError_t err = grad_alloc<R>(e, steps, K);
   if (err != cudaSuccess) return err;
   GradBuffers<R>& G = bufs<R>(e);
@@ -1368,7 +1370,8 @@ cudaError_t backward_impl(jf_engine* e, double* gparam_host) {
   if (err != cudaSuccess) return err;
   err = run_graph(e, bufs<R>(e).bwd_graph, graph_key<R>(e, 2), [&] { return bwd_record<R>(e); });
   if (err != cudaSuccess) return err;
-  return bwd_finish<R>(e, gparam_host);
+  if ((err = bwd_finish<R>(e, gparam_host)) == cudaSuccess) bufs<R>(e).have_backward = true;
+  return err;
 }
 
 // The loss sums into e->d_stats after a rollout: the engine's stats over its
@@ -1404,7 +1407,8 @@ cudaError_t step_impl(jf_engine* e, int64_t steps, int32_t K, const int32_t* bod
   if (err != cudaSuccess) return err;
   grad_advance_time(e, steps);
   bufs<R>(e).have_forward = true;
-  return bwd_finish<R>(e, gparam_host);
+  if ((err = bwd_finish<R>(e, gparam_host)) == cudaSuccess) bufs<R>(e).have_backward = true;
+  return err;
 }
 
 template <class R>
@@ -1451,4 +1455,13 @@ cudaError_t jf_grad_step_impl(jf_engine* e, int64_t steps, int32_t K, const int3
 // Position adjoint of the initial state for one instance, in engine order.
 cudaError_t jf_grad_x0_impl(jf_engine* e, int m, std::vector<float4>& out) {
   return fp64(e) ? x0_impl<double>(e, m, out) : x0_impl<float>(e, m, out);
+}
+
+// Whether the engine's latest rollout completed its forward (stage 1) or its
+// backward too (stage 2), in the engine's gradient precision.
+bool jf_grad_done(const jf_engine* e, int stage) {
+  if (!e->grad) return false;
+  const bool f = fp64(e) ? e->grad->f64.have_forward : e->grad->f32.have_forward;
+  const bool b = fp64(e) ? e->grad->f64.have_backward : e->grad->f32.have_backward;
+  return stage >= 2 ? (f && b) : f;
 }

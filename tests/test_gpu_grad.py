@@ -277,3 +277,35 @@ def test_grad_step_graph_matches_forward_and_backward():
             np.testing.assert_allclose(g[k], ref[1][k], rtol=1e-5)
         diff = np.abs(gx - ref[2])
         assert np.median(diff) <= 1e-6 * np.abs(ref[2]).max()
+
+
+def test_adjoint_queries_follow_the_latest_rollout():
+    """jf_grad_backward needs a completed forward and jf_grad_positions the
+    backward of the latest rollout: before them, and after a new forward,
+    they return JF_ERR_INVALID instead of a stale adjoint."""
+    from jellyfih_b200 import Engine, InstanceSpec
+    from jellyfih_b200 import _lib as L
+    pos, mat, fib, prm = grad_cases.small_tank(seed=6)
+    e = Engine([InstanceSpec(len(mat), 32, 32, 1.0)], path="plain")
+    e.load(0, pos, mat, fib)
+    e.set_params(actuation=[prm["actuation"]], contraction=[prm["contraction"]], freq=[prm["freq"]])
+    with pytest.raises(L.JfError, match="completed jf_grad_forward"):
+        e.grad_backward()
+    e.time = T0
+    e.grad_forward(10, 5)
+    with pytest.raises(L.JfError, match="latest rollout"):
+        e.grad_positions(0)
+    e.grad_backward()
+    gx = e.grad_positions(0)
+    assert gx.shape == (len(mat), 2) and np.all(np.isfinite(gx))
+    e.load(0, pos, mat, fib)
+    e.time = T0
+    e.grad_forward(10, 5)
+    with pytest.raises(L.JfError, match="latest rollout"):
+        e.grad_positions(0)
+    e.load(0, pos, mat, fib)
+    e.time = T0
+    e.grad_step(10, 5)
+    # the same rollout again: equal up to the adjoint's float-atomic order
+    assert np.median(np.abs(e.grad_positions(0) - gx)) <= 1e-6 * np.abs(gx).max()
+    e.close()

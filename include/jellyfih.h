@@ -188,8 +188,11 @@ int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, cons
  * actuation * g / (freq * dt) to d/d contraction and minus that times the
  * drop's time to d/d freq, g being d loss / d pressure at the drop.  The
  * reference engine has no gradients; this replaces nothing in it.  The engine
- * is left at the rollout's final state.  jf_grad_backward needs a completed
- * forward, and jf_grad_positions the backward of the latest rollout (a new
+ * is left at the rollout's final state, and so is it after jf_grad_backward,
+ * which recomputes the rollout from its checkpoints and puts that final
+ * particle state back (a state loaded or stepped in between is replaced; the
+ * time is not changed).  jf_grad_backward needs a completed forward, and
+ * jf_grad_positions the backward of the latest rollout (a new
  * jf_grad_forward discards the previous rollout's adjoint); otherwise they
  * return JF_ERR_INVALID. */
 int jf_grad_forward(jf_engine* e, int64_t steps, int32_t checkpoint_every, double* loss);

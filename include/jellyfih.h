@@ -86,7 +86,7 @@ int jf_create(const jf_config* cfg, jf_engine** out);
 int jf_destroy(jf_engine* e);
 /* Message of the engine's last failure; with e == NULL, of the calling
  * thread's last failed call made without a handle (jf_create,
- * jf_substep_noalloc).  The pointer stays valid until that engine's, or that
+ * jf_substep_noalloc, or any call given a NULL handle).  The pointer stays valid until that engine's, or that
  * thread's, next failure. */
 const char* jf_last_error(const jf_engine* e);
 const char* jf_version(void);

@@ -67,7 +67,17 @@ void free_particles(JfParticles& p) {
   p = JfParticles();
 }
 
-int check_engine(const jf_engine* e) { return e ? JF_OK : JF_ERR_INVALID; }
+// A call on a NULL handle fails with the thread's handle-less message set.
+int check_engine(const jf_engine* e) {
+  if (e) return JF_OK;
+  jf_set_global_error("NULL engine handle");
+  return JF_ERR_INVALID;
+}
+
+// JF_ERR_INVALID, with a message naming them, when required pointers are NULL.
+int need_args(jf_engine* e, bool present, const char* what) {
+  return present ? JF_OK : fail(e, JF_ERR_INVALID, std::string(what) + " must not be NULL");
+}
 
 int set_device(jf_engine* e) {
   JF_CK(cudaSetDevice(e->device), "cudaSetDevice");
@@ -656,21 +666,21 @@ int jf_sync_timeout(jf_engine* e, int64_t timeout_ms) {
 }
 
 int jf_payload_stats(jf_engine* e, double* out) {
-  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, out, "jf_payload_stats: out")) return JF_ERR_INVALID;
   int rc = set_device(e);
   if (rc) return rc;
   return stats_rows(e, out, false);
 }
 
 int jf_stats_any(jf_engine* e, double* out) {
-  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, out, "jf_stats_any: out")) return JF_ERR_INVALID;
   int rc = set_device(e);
   if (rc) return rc;
   return stats_rows(e, out, true);
 }
 
 int jf_stats_raw(jf_engine* e, double* out) {
-  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, out, "jf_stats_raw: out")) return JF_ERR_INVALID;
   int rc = set_device(e);
   if (rc) return rc;
   JF_CK(jf_stats_launch(e), "stats kernel");
@@ -681,7 +691,7 @@ int jf_stats_raw(jf_engine* e, double* out) {
 }
 
 int jf_run_headless(jf_engine* e, int64_t steps, double* out) {
-  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, out, "jf_run_headless: out")) return JF_ERR_INVALID;
   int rc = set_device(e);
   if (rc) return rc;
   e->t = 0.0f;
@@ -706,7 +716,8 @@ int jf_run_headless(jf_engine* e, int64_t steps, double* out) {
 
 int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts, const double* contraction,
                int32_t mode, double* out) {
-  if (check_engine(e) || !results || !muscle_counts || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, results && muscle_counts && out, "jf_fitness: results, muscle_counts and out"))
+    return JF_ERR_INVALID;
   if (mode != 0 && mode != 1) return fail(e, JF_ERR_INVALID, "fitness mode must be 0 or 1");
   int rc = set_device(e);
   if (rc) return rc;
@@ -728,7 +739,9 @@ int jf_fitness(jf_engine* e, const double* results, const int32_t* muscle_counts
 int jf_run_episode(jf_engine* e, const float* pos, const int32_t* material, const float* fiber,
                    const float* contraction, const float* freq, int64_t steps,
                    const int32_t* muscle_counts, int32_t mode, double* rows, double* fitness) {
-  if (check_engine(e) || !pos || !material || !contraction || !rows) return JF_ERR_INVALID;
+  if (check_engine(e) ||
+      need_args(e, pos && material && contraction && rows, "jf_run_episode: pos, material, contraction and rows"))
+    return JF_ERR_INVALID;
   if (steps < 0) return fail(e, JF_ERR_INVALID, "steps must be >= 0");
   if (muscle_counts && !fitness) return fail(e, JF_ERR_INVALID, "fitness output required with muscle_counts");
   if (mode != 0 && mode != 1) return fail(e, JF_ERR_INVALID, "fitness mode must be 0 or 1");
@@ -906,7 +919,7 @@ int jf_grad_backward(jf_engine* e, double* d_actuation, double* d_contraction, d
 }
 
 int jf_grad_positions(jf_engine* e, int32_t m, float* dx0) {
-  if (check_engine(e) || !dx0) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, dx0, "jf_grad_positions: dx0")) return JF_ERR_INVALID;
   if (m < 0 || m >= e->M) return fail(e, JF_ERR_INVALID, "instance index out of range");
   if (!jf_grad_done(e, 2))
     return fail(e, JF_ERR_INVALID,
@@ -994,7 +1007,7 @@ int jf_read_grid(jf_engine* e, int32_t m, float* grid_v, float* grid_m) {
 }
 
 int jf_error_flags(jf_engine* e, int32_t* out) {
-  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, out, "jf_error_flags: out")) return JF_ERR_INVALID;
   int rc = set_device(e);
   if (rc) return rc;
   JF_CK(cudaMemcpyAsync(out, e->d_err, sizeof(int32_t) * e->M, cudaMemcpyDeviceToHost, e->stream), "read flags");
@@ -1013,7 +1026,7 @@ int jf_clear_error_flags(jf_engine* e) {
 int64_t jf_kernel_launches(const jf_engine* e) { return e ? e->launches : -1; }
 
 int jf_path_counts(jf_engine* e, int64_t* out, int32_t reset) {
-  if (check_engine(e) || !out) return JF_ERR_INVALID;
+  if (check_engine(e) || need_args(e, out, "jf_path_counts: out")) return JF_ERR_INVALID;
   out[0] = out[1] = out[2] = out[3] = 0;
   if (!e->d_path) return JF_OK;
   int rc = set_device(e);

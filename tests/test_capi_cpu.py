@@ -56,6 +56,7 @@ def test_create_rejects_bad_config_before_touching_the_device(lib):
 
 def test_null_handle_calls_fail_cleanly(lib):
     assert lib.jf_step(None, 1) == L.JF_ERR_INVALID
+    assert lib.jf_last_error(None) == b"NULL engine handle"
     assert lib.jf_sync(None) == L.JF_ERR_INVALID
     assert lib.jf_sync_timeout(None, 10) == L.JF_ERR_INVALID
     assert lib.jf_payload_stats(None, None) == L.JF_ERR_INVALID

@@ -76,6 +76,8 @@ __host__ __device__ inline float jf_activation(float freq, float contraction, fl
   }
   return a;
 #else
+  // host: volatile stores keep every operation rounded on its own, as the
+  // device's __f*_rn do (no contraction into fused multiply-adds)
   volatile float period = 1.0f / (1.0f * freq);
   volatile float q = floorf(t / period);
   volatile float pq = period * q;

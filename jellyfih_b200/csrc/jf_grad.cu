@@ -1112,7 +1112,8 @@ cudaError_t fwd_record(jf_engine* e) {
 }
 
 // Phase of the waveform at time t as the rollout's precision computes it
-// (mpm_sim.py:173-174).
+// (mpm_sim.py:173-174); the volatile stores keep every operation rounded on
+// its own, as the device code does.
 float waveform_phase(float freq, float t) {
   volatile float period = 1.0f / (1.0f * freq);
   volatile float q = floorf(t / period);
